@@ -1,0 +1,198 @@
+/*
+ * reset.h -- C ABI of the B200-native RESET set-intersection library
+ * (libreset.so, sm_100a).
+ *
+ * Drop-in boundary for the reference's set-intersection path.  The reference
+ * has no FFI of its own: its entry points are C++ free functions over process
+ * globals, HashTableBuilder / *Baseline classes, and raw __global__ kernels.
+ * Each function below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - extern "C", plain pointers and sizes, int32 status returns; nothing
+ *    throws across the boundary.  reset_last_error_string() describes the
+ *    last failure on the calling host thread.
+ *  - Pointers prefixed d_ are device (HBM) pointers; h_ are host pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *    stream).  Calls are asynchronous on that stream except where noted.
+ *  - Tables use the reference layout: set u owns len[u] buckets of
+ *    `bucket` slots; slot k of bucket h of set u is
+ *        table[off[u] + h + k * bucket_num]        (int32, -1 = empty)
+ *    with bucket_num = sum(len) (triangle-count/hashtable.cu:53-76,
+ *    triangle-count/TC.cu:18).
+ *  - Handles are re-entrant: different tables may be used concurrently from
+ *    different threads/streams.  One table may be probed concurrently.
+ */
+#ifndef RESET_H
+#define RESET_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *reset_stream_t; /* cudaStream_t */
+
+typedef enum {
+  RESET_OK = 0,
+  RESET_ERR_CUDA = 1,        /* a CUDA runtime call failed */
+  RESET_ERR_OOM = 2,         /* device allocation failed */
+  RESET_ERR_ARG = 3,         /* invalid argument */
+  RESET_ERR_TABLE_FULL = 4,  /* a set does not fit its table (alpha > 1) */
+  RESET_ERR_PROBE_LIMIT = 5, /* a probe walked a whole table */
+  RESET_ERR_TIMEOUT = 6,     /* a bounded wait gave up */
+  RESET_ERR_UNSUPPORTED = 7, /* no sm_100 device / feature not built */
+  RESET_ERR_BUSY = 8         /* admission refused (serving) */
+} reset_status;
+
+#define RESET_ABI_VERSION 1
+
+/* Table parameters.  Defaults (reset_params_default): alpha = 0.2,
+ * bucket = 5, the reference defaults of triangle-count/TC.cu:220-221. */
+typedef struct reset_params {
+  float alpha;      /* load factor (0, 1]                                  */
+  int32_t bucket;   /* slots per bucket, 1..16                             */
+  int32_t reserved[6];
+} reset_params;
+
+void reset_params_default(reset_params *p);
+
+/* Opaque device-resident table (replaces the globals d_hash_table_*,
+ * d_hash_length, d_hash_tables_offset, max_length, bucket_num of
+ * triangle-count/TC.cuh:23-28 and the HashTableBuilder members of
+ * baseline/common/hash_table.cuh:82-94). */
+typedef struct reset_table reset_table;
+
+typedef struct reset_table_view {
+  int32_t n;            /* number of sets                                  */
+  int32_t bucket;       /* slots per bucket                                */
+  int32_t max_len;      /* maximum len over all sets                       */
+  int32_t hierarchical; /* 1: hierarchical hash, 0: normal hash            */
+  int64_t bucket_num;   /* total buckets = sum(len)                        */
+  int64_t m;            /* number of elements inserted                     */
+  float alpha;
+  int32_t pad;
+  int32_t *d_table;     /* bucket * bucket_num int32, slot-major           */
+  int32_t *d_len;       /* n                                               */
+  int64_t *d_off;       /* n + 1, d_off[n] == bucket_num                   */
+} reset_table_view;
+
+/* Build one table over the sets of a CSR (d_off[n+1] int32, d_elems[m]
+ * int32, element ids >= 0).  Replaces make_hash_table
+ * (triangle-count/hashtable.cu:103-183; set-similarity-search/
+ * hashtable.cu:100-181; information-retrieval/hashtable.cu:162-249) and
+ * HashTableBuilder::build_hash_tables (baseline/common/hash_table.cu:69-192)
+ * for one hash function at a time.  len/off/bucket_num/max_len follow
+ * calculate_length (triangle-count/hashtable.cu:21-36) exactly.  Keys are
+ * placed by the reference insertion rule (hashtable.cu:53-101) applied in
+ * CSR order, so the layout is deterministic.  Synchronises `stream` once
+ * (to size the table).  If d_hash_order_out is not NULL it receives, in the
+ * same pass, every row read back in bucket order (what
+ * launch_extract_hashtable_to_csr, baseline/common/utils.cu:148-175,
+ * produces). */
+reset_status reset_table_build(const int32_t *d_off, const int32_t *d_elems,
+                               int32_t n, int64_t m, const reset_params *params,
+                               int32_t hierarchical, int32_t *d_hash_order_out,
+                               reset_table **out, reset_stream_t stream);
+
+/* Device pointers and sizes of a table (for dumps and for callers that
+ * launch their own kernels over the reference layout).  Host-only. */
+reset_status reset_table_info(const reset_table *t, reset_table_view *view);
+
+/* Free a table (replaces HashTableBuilder::free_hash_tables,
+ * baseline/common/hash_table.cuh:45-72).  Synchronises the device. */
+reset_status reset_table_free(reset_table *t);
+
+/* Synchronise `stream` and report device-side errors raised by kernels that
+ * used this table since the last call (RESET_ERR_PROBE_LIMIT,
+ * RESET_ERR_TABLE_FULL), then clear them. */
+reset_status reset_table_check(reset_table *t, reset_stream_t stream);
+
+/* Rows of the table's CSR read back in bucket order (slot-major within each
+ * set, -1 dropped).  Replaces launch_extract_hashtable_to_csr
+ * (baseline/common/utils.cu:148-175) and the sort by column % max_length
+ * of gpu_sort_csr_cols (triangle-count/TC.cu:107-126). */
+reset_status reset_csr_hash_order(const reset_table *t, const int32_t *d_off,
+                                  int32_t *d_cols_out, reset_stream_t stream);
+
+/* Triangle count over an oriented CSR whose table is `t`:
+ *   sum over edges e=(u, d_cols[e]) of |row(u) ∩ row(v)|,
+ * the smaller row's keys probed into the larger row's table.  d_cols may be
+ * the plain rows or the hash-ordered rows.  *d_count (device u64) is
+ * overwritten.  Replaces dynamic_triangle_count (triangle-count/TC.cu:128-190)
+ * and TCBaseline::run_{normal,hierarchical} (baseline/tc/tc.cu:165-237). */
+reset_status reset_tc_count(const reset_table *t, const int32_t *d_off,
+                            const int32_t *d_cols, int64_t m,
+                            uint64_t *d_count, reset_stream_t stream);
+
+/* Set-similarity decisions for P explicit pairs (d_pair_a[p], d_pair_b[p])
+ * of sets of the table's CSR.  I = |A ∩ B| by probing the smaller set into
+ * the larger set's table; U = |A| + |B| - I.
+ *   d_flags[p] = U > 0 && den * I >= num * U            (exact, integer)
+ * d_inter (optional) receives I.  Replaces set_similarity_search_kernel
+ * (set-similarity-search/sss.cu:93-154) and SSSBaseline::run_*
+ * (baseline/sss/sss.cu:145-251), whose float rule
+ * I / (float)U >= thr is available through reset_sss_float. */
+reset_status reset_sss(const reset_table *t, const int32_t *d_off,
+                       const int32_t *d_elems, const int32_t *d_pair_a,
+                       const int32_t *d_pair_b, int64_t npairs, int32_t num,
+                       int32_t den, uint8_t *d_flags, int32_t *d_inter,
+                       reset_stream_t stream);
+
+/* The reference's float decision, bit-exact with sss.cu:139-141:
+ *   d_flags[p] = (float)I / (float)U >= thr. */
+reset_status reset_sss_float(const reset_table *t, const int32_t *d_off,
+                             const int32_t *d_elems, const int32_t *d_pair_a,
+                             const int32_t *d_pair_b, int64_t npairs,
+                             float thr, uint8_t *d_flags, int32_t *d_inter,
+                             reset_stream_t stream);
+
+/* Conjunctive retrieval.  The table is built over the inverted index
+ * (d_toff[nterms+1], d_docs).  Query q is the term list
+ * d_query[d_qoff[q] .. d_qoff[q+1]); its result is the posting list of its
+ * first term, in d_docs order, filtered by membership in every further
+ * term's table.  Survivors go to d_res[d_res_off[q] ...] (the caller sizes
+ * slot q for df(first term), as ir.cu:324-330 does); d_cnt[q] receives the
+ * count.  Empty queries yield 0.  Replaces ir_kernel
+ * (information-retrieval/ir.cu:94-176) and IRBaseline::run_*
+ * (baseline/ir/ir.cu:240-343). */
+reset_status reset_ir(const reset_table *t, const int32_t *d_toff,
+                      const int32_t *d_docs, const int32_t *d_query,
+                      const int32_t *d_qoff, int32_t nq,
+                      const int64_t *d_res_off, int32_t *d_res,
+                      int32_t *d_cnt, reset_stream_t stream);
+
+/* |A ∩ B| counted with A's multiplicity for one pair of device arrays
+ * (keys >= 0).  Builds B's table with `params` and probes A.  *d_count
+ * (device i64) is overwritten.  Replaces make_hashtable_kernel +
+ * intersection_kernel (set_size/intersection.cu:128-181). */
+reset_status reset_intersect_count(const int32_t *d_a, int64_t na,
+                                   const int32_t *d_b, int64_t nb,
+                                   const reset_params *params,
+                                   int64_t *d_count, reset_stream_t stream);
+
+/* ---- synthetic inputs (stand-ins for the reference's datasets) -------- */
+
+/* Seeded R-MAT graph on the device: 2^scale vertices, edge_factor*2^scale
+ * generated edges; self-loops and duplicates removed, symmetrised.
+ * oriented = 1: keep u->v iff (deg u, u) < (deg v, v) (triangle-counting
+ * input); oriented = 0: full symmetric adjacency.  Rows sorted ascending.
+ * Outputs are allocated with cudaMalloc and owned by the caller (free with
+ * reset_free).  Synchronises `stream`. */
+reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed,
+                            double a, double b, double c, int32_t oriented,
+                            int32_t **d_off_out, int32_t **d_cols_out,
+                            int64_t *m_out, reset_stream_t stream);
+reset_status reset_free(void *d_ptr);
+
+/* ---- misc --------------------------------------------------------------- */
+
+const char *reset_last_error_string(void);
+const char *reset_status_string(int32_t status);
+int32_t reset_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RESET_H */

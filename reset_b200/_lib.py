@@ -1,0 +1,92 @@
+"""ctypes binding of libreset.so (the C ABI declared in include/reset.h).
+
+The library is loaded from this package directory.  There is no fallback:
+if libreset.so is missing or cannot be loaded, importing the bindings
+raises, so no code path silently runs without the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libreset.so")
+
+STATUS = {
+    0: "RESET_OK", 1: "RESET_ERR_CUDA", 2: "RESET_ERR_OOM", 3: "RESET_ERR_ARG",
+    4: "RESET_ERR_TABLE_FULL", 5: "RESET_ERR_PROBE_LIMIT",
+    6: "RESET_ERR_TIMEOUT", 7: "RESET_ERR_UNSUPPORTED", 8: "RESET_ERR_BUSY",
+}
+
+
+class ResetError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("bucket", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class TableView(C.Structure):
+    _fields_ = [("n", C.c_int32), ("bucket", C.c_int32), ("max_len", C.c_int32),
+                ("hierarchical", C.c_int32), ("bucket_num", C.c_int64),
+                ("m", C.c_int64), ("alpha", C.c_float), ("pad", C.c_int32),
+                ("d_table", C.c_void_p), ("d_len", C.c_void_p),
+                ("d_off", C.c_void_p)]
+
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+
+# name -> (restype, argtypes); every symbol include/reset.h declares.
+SIGNATURES = {
+    "reset_params_default": (None, [C.POINTER(Params)]),
+    "reset_table_build": (I32, [P, P, I32, I64, C.POINTER(Params), I32, P,
+                                C.POINTER(P), P]),
+    "reset_table_info": (I32, [P, C.POINTER(TableView)]),
+    "reset_table_free": (I32, [P]),
+    "reset_table_check": (I32, [P, P]),
+    "reset_csr_hash_order": (I32, [P, P, P, P]),
+    "reset_tc_count": (I32, [P, P, P, I64, P, P]),
+    "reset_sss": (I32, [P, P, P, P, P, I64, I32, I32, P, P, P]),
+    "reset_sss_float": (I32, [P, P, P, P, P, I64, C.c_float, P, P, P]),
+    "reset_ir": (I32, [P, P, P, P, P, I32, P, P, P, P]),
+    "reset_intersect_count": (I32, [P, I64, P, I64, C.POINTER(Params), P, P]),
+    "reset_gen_rmat": (I32, [I32, I32, C.c_uint64, C.c_double, C.c_double,
+                             C.c_double, I32, C.POINTER(P), C.POINTER(P),
+                             C.POINTER(I64), P]),
+    "reset_free": (I32, [P]),
+    "reset_last_error_string": (C.c_char_p, []),
+    "reset_status_string": (C.c_char_p, [I32]),
+    "reset_abi_version": (I32, []),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libreset.so and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"libreset.so not found at {path}; build it with "
+            "`python -m reset_b200.build` (there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int):
+    if status != 0:
+        msg = load().reset_last_error_string()
+        raise ResetError(status, msg.decode() if msg else "")

@@ -1,0 +1,224 @@
+"""Python host API over the C ABI (include/reset.h).
+
+Device buffers are torch CUDA tensors (plumbing only); every computation
+runs in libreset.so.  Functions take and return int32/int64 tensors on the
+current CUDA device and run on the current torch stream unless `stream` is
+given.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Tuple
+
+import torch
+
+from ._lib import Params, TableView, check, load
+
+
+def _lib():
+    return load()
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _need(t: torch.Tensor, dtype, name: str):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t
+
+
+class _CudaArray:
+    """Zero-copy view of a device pointer (__cuda_array_interface__ v3)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {
+            "shape": (int(n),), "typestr": typestr, "data": (int(ptr or 0), False),
+            "version": 3, "strides": None}
+
+
+def _view(ptr, n, dtype) -> torch.Tensor:
+    typestr = {torch.int32: "<i4", torch.int64: "<i8"}[dtype]
+    if n == 0:
+        return torch.empty(0, dtype=dtype, device="cuda")
+    return torch.as_tensor(_CudaArray(ptr, n, typestr), device="cuda")
+
+
+def params(alpha: float = 0.2, bucket: int = 5) -> Params:
+    p = Params()
+    _lib().reset_params_default(C.byref(p))
+    p.alpha = alpha
+    p.bucket = bucket
+    return p
+
+
+class Table:
+    """A device-resident table over the sets (rows) of a CSR.
+
+    Mirrors one half of HashTableBuilder (baseline/common/hash_table.cuh:12-95):
+    build with (load factor, bucket size, hash function), read back len /
+    offsets / slots, free.  With hash_order=True the rows read back in bucket
+    order are produced in the same pass (``self.hash_order``).
+    """
+
+    def __init__(self, off: torch.Tensor, elems: torch.Tensor, alpha: float = 0.2,
+                 bucket: int = 5, hierarchical: bool = True, hash_order: bool = False,
+                 stream=None):
+        self.off = _need(off, torch.int32, "off")
+        self.elems = _need(elems, torch.int32, "elems")
+        self.n = off.numel() - 1
+        self.m = elems.numel()
+        self.hash_order = torch.empty_like(elems) if hash_order else None
+        h = C.c_void_p()
+        p = params(alpha, bucket)
+        check(_lib().reset_table_build(_ptr(off), _ptr(elems), self.n, self.m,
+                                       C.byref(p), int(bool(hierarchical)),
+                                       _ptr(self.hash_order), C.byref(h),
+                                       _stream(stream)))
+        self._h = h
+        v = TableView()
+        check(_lib().reset_table_info(h, C.byref(v)))
+        self.bucket = v.bucket
+        self.max_len = v.max_len
+        self.hierarchical = bool(v.hierarchical)
+        self.bucket_num = v.bucket_num
+        self.alpha = v.alpha
+        self._v = v
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("table already freed")
+        return self._h
+
+    def tensors(self) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """Zero-copy (slots, len, off) views; valid while the table lives."""
+        v = self._v
+        return (_view(v.d_table, self.bucket * self.bucket_num, torch.int32),
+                _view(v.d_len, self.n, torch.int32),
+                _view(v.d_off, self.n + 1, torch.int64))
+
+    def check(self, stream=None):
+        check(_lib().reset_table_check(self.handle, _stream(stream)))
+
+    def csr_hash_order(self, off: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        off = self.off if off is None else _need(off, torch.int32, "off")
+        out = torch.empty(self.m, dtype=torch.int32, device=self.off.device)
+        check(_lib().reset_csr_hash_order(self.handle, _ptr(off), _ptr(out), _stream(stream)))
+        return out
+
+    def free(self):
+        if self._h is not None:
+            check(_lib().reset_table_free(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None) is not None:
+                _lib().reset_table_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def tc_count_async(t: Table, off: torch.Tensor, cols: torch.Tensor,
+                   out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+    """Triangle count into a device u64 (as int64 tensor), asynchronously."""
+    if out is None:
+        out = torch.empty(1, dtype=torch.int64, device=cols.device)
+    check(_lib().reset_tc_count(t.handle, _ptr(off), _ptr(cols), cols.numel(),
+                                _ptr(out), _stream(stream)))
+    return out
+
+
+def tc_count(t: Table, off: torch.Tensor, cols: torch.Tensor, stream=None) -> int:
+    out = tc_count_async(t, off, cols, stream=stream)
+    return int(out.item()) & ((1 << 64) - 1)
+
+
+def sss(t: Table, off, elems, pa, pb, num: int = 7, den: int = 10,
+        with_inter: bool = True, stream=None):
+    """Integer-rule set-similarity decisions -> (flags uint8, inter int32)."""
+    P = pa.numel()
+    flags = torch.empty(P, dtype=torch.uint8, device=pa.device)
+    inter = torch.empty(P, dtype=torch.int32, device=pa.device) if with_inter else None
+    check(_lib().reset_sss(t.handle, _ptr(off), _ptr(elems), _ptr(pa), _ptr(pb), P,
+                           num, den, _ptr(flags), _ptr(inter), _stream(stream)))
+    return flags, inter
+
+
+def sss_float(t: Table, off, elems, pa, pb, thr: float, with_inter: bool = True,
+              stream=None):
+    """Reference float-rule decisions (sss.cu:139-141) -> (flags, inter)."""
+    P = pa.numel()
+    flags = torch.empty(P, dtype=torch.uint8, device=pa.device)
+    inter = torch.empty(P, dtype=torch.int32, device=pa.device) if with_inter else None
+    check(_lib().reset_sss_float(t.handle, _ptr(off), _ptr(elems), _ptr(pa), _ptr(pb),
+                                 P, C.c_float(thr), _ptr(flags), _ptr(inter),
+                                 _stream(stream)))
+    return flags, inter
+
+
+def ir_result_offsets(toff: torch.Tensor, query: torch.Tensor, qoff: torch.Tensor) -> torch.Tensor:
+    """res_off[q+1] = res_off[q] + df(first term of q) (ir.cu:324-330); 0 for
+    empty queries.  Plain tensor arithmetic (input plumbing)."""
+    Q = qoff.numel() - 1
+    ql = qoff[1:] - qoff[:-1]
+    first = query[qoff[:-1].clamp(max=max(query.numel() - 1, 0)).long()] if query.numel() else \
+        torch.zeros(Q, dtype=torch.int32, device=qoff.device)
+    df = (toff[first.long() + 1] - toff[first.long()]).to(torch.int64)
+    df = torch.where(ql > 0, df, torch.zeros_like(df))
+    roff = torch.zeros(Q + 1, dtype=torch.int64, device=qoff.device)
+    roff[1:] = torch.cumsum(df, 0)
+    return roff
+
+
+def ir(t: Table, toff, docs, query, qoff, res_off=None, stream=None):
+    """Conjunctive retrieval -> (res_off int64[Q+1], res int32, cnt int32[Q])."""
+    Q = qoff.numel() - 1
+    if res_off is None:
+        res_off = ir_result_offsets(toff, query, qoff)
+    total = int(res_off[-1].item()) if Q > 0 else 0
+    res = torch.full((max(total, 1),), -1, dtype=torch.int32, device=docs.device)
+    cnt = torch.zeros(max(Q, 1), dtype=torch.int32, device=docs.device)
+    check(_lib().reset_ir(t.handle, _ptr(toff), _ptr(docs), _ptr(query), _ptr(qoff), Q,
+                          _ptr(res_off), _ptr(res), _ptr(cnt), _stream(stream)))
+    return res_off, res[:total], cnt[:Q]
+
+
+def intersect_count(a: torch.Tensor, b: torch.Tensor, alpha: float = 0.2,
+                    bucket: int = 5, stream=None) -> int:
+    out = torch.zeros(1, dtype=torch.int64, device=a.device)
+    p = params(alpha, bucket)
+    check(_lib().reset_intersect_count(_ptr(a), a.numel(), _ptr(b), b.numel(),
+                                       C.byref(p), _ptr(out), _stream(stream)))
+    return int(out.item())
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 0x5EED0016,
+             a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             oriented: bool = True, stream=None):
+    """Seeded R-MAT CSR generated on the device -> (off int32, cols int32)."""
+    L = _lib()
+    po, pc, m = C.c_void_p(), C.c_void_p(), C.c_int64()
+    check(L.reset_gen_rmat(scale, edge_factor, seed, a, b, c, int(bool(oriented)),
+                           C.byref(po), C.byref(pc), C.byref(m), _stream(stream)))
+    try:
+        n = 1 << scale
+        off = _view(po.value, n + 1, torch.int32).clone()
+        cols = _view(pc.value, m.value, torch.int32).clone()
+        torch.cuda.current_stream().synchronize()
+    finally:
+        L.reset_free(po)
+        L.reset_free(pc)
+    return off, cols

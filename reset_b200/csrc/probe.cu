@@ -1,0 +1,612 @@
+// Hash-probe intersection kernels: triangle counting, set-similarity search,
+// the raw two-set intersection, and conjunctive retrieval.
+//
+// Reference kernels: dynamic_triangle_count (triangle-count/TC.cu:128-190),
+// set_similarity_search_kernel (set-similarity-search/sss.cu:93-154),
+// intersection_kernel (set_size/intersection.cu:154-181), ir_kernel
+// (information-retrieval/ir.cu:94-176).  All share the probe rule of
+// search_in_hashtable (TC.cu:11-31): walk the slots of the home bucket, then
+// the next bucket; a hit is an equal slot, a miss an empty (-1) slot.
+//
+// Scheduling (B200): the reference gives every pair a whole warp, so a warp
+// probing a 3-element set idles 29 lanes.  Here a warp takes 32 pairs (one
+// per lane), loads each pair's two packed 16-byte set descriptors, and
+// flattens the probes of all 32 pairs: round r gives lane i the probe with
+// flat index 32r+i, found by a 5-step shuffle binary search over the pairs'
+// prefix sums.  Tiny intersections thus run at thread granularity, medium
+// ones spread over the warp, and hub x hub pairs over as many rounds as
+// they need; the grid is persistent and walks 32-pair chunks grid-stride.
+#include <cub/cub.cuh>
+
+#include <climits>
+
+#include "common.cuh"
+
+namespace rst {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kIrSlice = 2048;  // candidates per IR work item
+
+enum : int32_t { kErrBadId = 4 };
+
+template <bool HIER>
+__device__ __forceinline__ bool probe_key(int x, const int32_t* __restrict__ tb,
+                                          int lg, int lg_max, int64_t bn,
+                                          int b, int32_t* status) {
+  const int l = 1 << lg;
+  int h = home_bucket<HIER>(x, lg, lg_max);
+  int k = 0;
+  const int64_t cap = (int64_t)l * b;
+  for (int64_t t = 0; t < cap; ++t) {
+    const int s = __ldg(tb + h + (int64_t)k * bn);
+    if (s == x) return true;
+    if (s == -1) return false;
+    if (++k == b) {
+      k = 0;
+      h = (h + 1) & (l - 1);
+    }
+  }
+  atomicOr(status, kErrProbeLimit);
+  return false;
+}
+
+// Warp-inclusive scan; returns the exclusive prefix and sets *total.
+__device__ __forceinline__ int warp_excl_scan(int s, int* total) {
+  const int lane = threadIdx.x & 31;
+  int incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  *total = __shfl_sync(kFull, incl, 31);
+  return incl - s;
+}
+
+// Largest lane k with P_k <= f (P nondecreasing across lanes, P_0 = 0).
+__device__ __forceinline__ int owner_lane(int P, int f) {
+  int k = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    int pk = __shfl_sync(kFull, P, k + step);
+    if (pk <= f) k += step;
+  }
+  return k;
+}
+
+// Row of edge e (warp-collective).  u0 is the row of the chunk's first edge;
+// row(e) = u0 + #{j : off[u0+1+j] <= e}, searched 32 rows at a time.
+__device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
+                                           int n, int u0, int e) {
+  const int lane = threadIdx.x & 31;
+  int row = -1;
+  for (int ub = u0;; ub += 32) {
+    const int idx = ub + 1 + lane;
+    const int q = idx <= n ? __ldg(off + idx) : INT_MAX;
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      int qq = __shfl_sync(kFull, q, c + step - 1);
+      if (qq <= e) c += step;
+    }
+    const int q31 = __shfl_sync(kFull, q, 31);
+    if (c == 31 && q31 <= e) c = 32;
+    if (row < 0 && c < 32) row = ub + c;
+    if (__all_sync(kFull, row >= 0)) break;
+  }
+  return row;
+}
+
+// Flattened probing of 32 (probe side, table side) pairs held one per lane.
+// For every hit, on_hit(k) is called on the lane that probed, with k the
+// lane index of the owning pair.
+template <bool HIER, class OnHit>
+__device__ __forceinline__ void flat_probe(const int32_t* __restrict__ keys,
+                                           const int32_t* __restrict__ table,
+                                           int s, int a_start, int64_t toff,
+                                           int lg, int lg_max, int64_t bn,
+                                           int b, int32_t* status,
+                                           OnHit on_hit) {
+  const int lane = threadIdx.x & 31;
+  int S;
+  const int P = warp_excl_scan(s, &S);
+  for (int base = 0; base < S; base += 32) {
+    const int f = base + lane;
+    const int k = owner_lane(P, f);
+    const int kp = __shfl_sync(kFull, P, k);
+    const int ka = __shfl_sync(kFull, a_start, k);
+    const int klg = __shfl_sync(kFull, lg, k);
+    const int64_t kt = __shfl_sync(kFull, toff, k);
+    if (f < S) {
+      const int x = __ldg(keys + ka + (f - kp));
+      if (probe_key<HIER>(x, table + kt, klg, lg_max, bn, b, status)) on_hit(k);
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+  return v;
+}
+
+// ----------------------------------------------------------------- TC ----
+
+template <bool HIER>
+__global__ void __launch_bounds__(kThreads)
+    tc_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ off,
+              const int32_t* __restrict__ cols,
+              const int32_t* __restrict__ chunk_row, int32_t n, int64_t m,
+              const int32_t* __restrict__ table, int64_t bn, int b, int lg_max,
+              unsigned long long* __restrict__ count,
+              int32_t* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  // edges past off[n] have no row: never read them (nor their chunk rows)
+  const int64_t me = min(m, (int64_t)__ldg(off + n));
+  const int64_t n_chunks = (me + 31) >> 5;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long hits = 0;
+  for (int64_t c = gw; c < n_chunks; c += nw) {
+    const int64_t e64 = c * 32 + lane;
+    const bool valid = e64 < me;
+    const int e = (int)(valid ? e64 : me - 1);
+    int u0 = __ldg(chunk_row + c);
+    if ((unsigned)u0 >= (unsigned)n) u0 = 0;
+    int u = row_of_edge(off, n, u0, e);
+    int v = __ldg(cols + e);
+    bool ok = valid;
+    if ((unsigned)u >= (unsigned)n || (unsigned)v >= (unsigned)n) {
+      if (valid) atomicOr(status, kErrBadId);
+      ok = false;
+      u = v = 0;
+    }
+    const int4 du = __ldg(desc + u);
+    const int4 dv = __ldg(desc + v);
+    // TC.cu:148-157: the larger set's table is probed (ties: u probes v).
+    const bool sw = du.y > dv.y;
+    const int4 A = sw ? dv : du;
+    const int4 B = sw ? du : dv;
+    const int s = ok ? A.y : 0;
+    flat_probe<HIER>(cols, table, s, A.x, desc_toff(B), desc_lg(B), lg_max, bn,
+                     b, status, [&](int) { ++hits; });
+  }
+  hits = warp_sum_u64(hits);
+  if (lane == 0 && hits) atomicAdd(count, hits);
+}
+
+// ---------------------------------------------------------------- SSS ----
+
+template <bool HIER, bool FLOAT_RULE>
+__global__ void __launch_bounds__(kThreads)
+    sss_kernel(const int4* __restrict__ desc, int32_t n,
+               const int32_t* __restrict__ elems,
+               const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
+               int64_t np, const int32_t* __restrict__ table, int64_t bn, int b,
+               int lg_max, int num, int den, float thr,
+               uint8_t* __restrict__ flags, int32_t* __restrict__ inter,
+               int32_t* __restrict__ status) {
+  __shared__ int s_hits[kWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t n_chunks = (np + 31) >> 5;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t c = gw; c < n_chunks; c += nw) {
+    const int64_t p = c * 32 + lane;
+    const bool valid = p < np;
+    int a = valid ? __ldg(pa + p) : 0;
+    int q = valid ? __ldg(pb + p) : 0;
+    bool ok = valid;
+    if ((unsigned)a >= (unsigned)n || (unsigned)q >= (unsigned)n) {
+      if (valid) atomicOr(status, kErrBadId);
+      ok = false;
+      a = q = 0;
+    }
+    const int4 da = __ldg(desc + a);
+    const int4 dq = __ldg(desc + q);
+    const bool sw = da.y > dq.y;  // sss.cu:108-115
+    const int4 A = sw ? dq : da;
+    const int4 B = sw ? da : dq;
+    s_hits[warp][lane] = 0;
+    __syncwarp();
+    flat_probe<HIER>(elems, table, ok ? A.y : 0, A.x, desc_toff(B),
+                     desc_lg(B), lg_max, bn, b, status,
+                     [&](int k) { atomicAdd(&s_hits[warp][k], 1); });
+    __syncwarp();
+    const int I = s_hits[warp][lane];
+    __syncwarp();
+    if (ok) {
+      const int U = da.y + dq.y - I;
+      bool f;
+      if (FLOAT_RULE) {
+        f = ((float)I / (float)U) >= thr;  // sss.cu:139-140
+      } else {
+        f = U > 0 && (int64_t)den * I >= (int64_t)num * U;
+      }
+      flags[p] = (uint8_t)f;
+      if (inter) inter[p] = I;
+    } else if (valid) {
+      flags[p] = 0;
+      if (inter) inter[p] = 0;
+    }
+  }
+}
+
+// ----------------------------------------------------------- raw pair ----
+
+__global__ void __launch_bounds__(kThreads)
+    pair_probe_kernel(const int32_t* __restrict__ a, int64_t na,
+                      const int32_t* __restrict__ table, int lg, int64_t bn,
+                      int b, unsigned long long* __restrict__ count,
+                      int32_t* __restrict__ status) {
+  unsigned long long hits = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < na;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    // set_size/intersection.cu:169: d_hash(key, len) = key & (len-1)
+    hits += probe_key<false>(__ldg(a + i), table, lg, lg, bn, b, status);
+  }
+  hits = warp_sum_u64(hits);
+  if ((threadIdx.x & 31) == 0 && hits) atomicAdd(count, hits);
+}
+
+// ----------------------------------------------------------------- IR ----
+
+__global__ void ir_plan_kernel(const int4* __restrict__ desc, int32_t n,
+                               const int32_t* __restrict__ query,
+                               const int32_t* __restrict__ qoff, int32_t nq,
+                               int64_t* __restrict__ sl_off,
+                               int32_t* __restrict__ status) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int qs = qoff[q], ql = qoff[q + 1] - qs;
+    int64_t ns = 0;
+    if (ql > 0) {
+      const int t0 = query[qs];
+      if ((unsigned)t0 < (unsigned)n) {
+        const int df = desc[t0].y;
+        ns = (df + kIrSlice - 1) / kIrSlice;
+      } else {
+        atomicOr(status, kErrBadId);
+      }
+    }
+    sl_off[q] = ns;
+  }
+}
+
+__global__ void ir_total_kernel(const int64_t* __restrict__ ns_excl,
+                                int64_t* __restrict__ sl_off, int32_t nq,
+                                int64_t* __restrict__ total) {
+  // sl_off holds the exclusive scan of the slice counts for q < nq; the
+  // count of the last query is recomputed by the caller into ns_excl[0].
+  int64_t t = nq > 0 ? sl_off[nq - 1] + ns_excl[0] : 0;
+  sl_off[nq] = t;
+  *total = t;
+}
+
+// One warp per slice of kIrSlice candidates of the first term's list:
+// every candidate is checked against all further terms (early exit per
+// lane), survivors are compacted with ballot/popc to the front of the
+// slice's own region of the result buffer, in first-term order.
+template <bool HIER>
+__global__ void __launch_bounds__(kThreads)
+    ir_slice_kernel(const int4* __restrict__ desc, int32_t n,
+                    const int32_t* __restrict__ docs,
+                    const int32_t* __restrict__ query,
+                    const int32_t* __restrict__ qoff, int32_t nq,
+                    const int64_t* __restrict__ sl_off,
+                    const int64_t* __restrict__ res_off,
+                    int32_t* __restrict__ res, int32_t* __restrict__ sl_cnt,
+                    const int32_t* __restrict__ table, int64_t bn, int b,
+                    int lg_max, int32_t* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const int64_t total = sl_off[nq];
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sidx = gw; sidx < total; sidx += nw) {
+    // query owning this slice: largest q with sl_off[q] <= sidx
+    int lo = 0, hi = nq - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (sl_off[mid] <= sidx) lo = mid; else hi = mid - 1;
+    }
+    const int q = lo;
+    const int qs = qoff[q], ql = qoff[q + 1] - qs;
+    const int4 d0 = desc[query[qs]];
+    const int64_t j0 = (sidx - sl_off[q]) * kIrSlice;
+    const int64_t j1 = min((int64_t)d0.y, j0 + kIrSlice);
+    int32_t* out = res + res_off[q] + j0;
+    int w = 0;
+    for (int64_t jb = j0; jb < j1; jb += 32) {
+      const int64_t j = jb + lane;
+      const bool active = j < j1;
+      const int x = active ? __ldg(docs + d0.x + j) : 0;
+      bool ok = active;
+      for (int i = 1; i < ql; ++i) {  // ir.cu:131-161, all terms per candidate
+        const int t = __ldg(query + qs + i);
+        if ((unsigned)t >= (unsigned)n) {
+          if (ok) atomicOr(status, kErrBadId);
+          ok = false;
+          continue;
+        }
+        if (!__any_sync(kFull, ok)) break;
+        const int4 dt = __ldg(desc + t);
+        if (ok)
+          ok = probe_key<HIER>(x, table + desc_toff(dt), desc_lg(dt), lg_max,
+                               bn, b, status);
+      }
+      const unsigned msk = __ballot_sync(kFull, ok);
+      if (ok) out[w + __popc(msk & lt)] = x;
+      w += __popc(msk);
+    }
+    if (lane == 0) sl_cnt[sidx] = w;
+  }
+}
+
+// One warp per query: slides the survivors of slices 1.. down behind those
+// of slice 0 (destination never past the source) and writes the count.
+__global__ void __launch_bounds__(kThreads)
+    ir_compact_kernel(const int64_t* __restrict__ sl_off, int32_t nq,
+                      const int64_t* __restrict__ res_off,
+                      int32_t* __restrict__ res,
+                      const int32_t* __restrict__ sl_cnt,
+                      int32_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t q = gw; q < nq; q += nw) {
+    const int64_t s0 = sl_off[q], ns = sl_off[q + 1] - s0;
+    int32_t* base = res + res_off[q];
+    int64_t tot = ns > 0 ? sl_cnt[s0] : 0;
+    for (int64_t i = 1; i < ns; ++i) {
+      const int c = sl_cnt[s0 + i];
+      const int32_t* src = base + i * kIrSlice;
+      int32_t* dst = base + tot;
+      for (int j = 0; j < c; j += 32) {
+        int v = 0;
+        if (j + lane < c) v = src[j + lane];
+        __syncwarp();
+        if (j + lane < c) dst[j + lane] = v;
+        __syncwarp();
+      }
+      tot += c;
+    }
+    if (lane == 0) cnt[q] = (int32_t)tot;
+  }
+}
+
+int persistent_grid(const void* kernel) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0);
+  if (per_sm < 1) per_sm = 1;
+  return sm_count() * per_sm;
+}
+
+int64_t clamp_grid(int64_t want, int cap) {
+  if (want < 1) want = 1;
+  return want < cap ? want : cap;
+}
+
+// Resolves the descriptor array for a probe call: the table's own when the
+// caller passes the offsets the table was built on, else a fresh one.
+struct DescScope {
+  const int4* desc = nullptr;
+  int4* owned = nullptr;
+  cudaStream_t st = nullptr;
+  ~DescScope() {
+    if (owned) cudaFreeAsync(owned, st);
+  }
+};
+
+reset_status resolve_desc(const reset_table* t, const int32_t* d_off,
+                          cudaStream_t st, DescScope* ds) {
+  ds->st = st;
+  if (!d_off || d_off == t->build_off) {
+    ds->desc = t->d_desc;
+    return RESET_OK;
+  }
+  RST_CHECK(make_desc(t, d_off, &ds->owned, st));
+  ds->desc = ds->owned;
+  return RESET_OK;
+}
+
+}  // namespace
+}  // namespace rst
+
+using namespace rst;
+
+extern "C" {
+
+reset_status reset_tc_count(const reset_table* t, const int32_t* d_off,
+                            const int32_t* d_cols, int64_t m,
+                            uint64_t* d_count, reset_stream_t stream) {
+  if (!t || !d_count) return arg_fail("NULL table or count");
+  if (m < 0 || m > INT32_MAX) return arg_fail("m out of range");
+  if (m > 0 && (!d_cols || !d_off)) return arg_fail("NULL offsets or cols");
+  cudaStream_t st = as_stream(stream);
+  RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
+  if (m == 0 || t->n == 0) return RESET_OK;
+  DescScope ds;
+  RST_CHECK(resolve_desc(t, d_off, st, &ds));
+  const int32_t* rows = t->d_chunk_row;
+  int32_t* owned_rows = nullptr;
+  if (d_off != t->build_off || m != t->m) {
+    RST_CHECK(make_chunk_rows(d_off, t->n, m, &owned_rows, st));
+    rows = owned_rows;
+  }
+  const void* k = t->hier ? (const void*)tc_kernel<true> : (const void*)tc_kernel<false>;
+  const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps, persistent_grid(k));
+  if (t->hier)
+    tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
+        ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
+        t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
+        t->d_status);
+  else
+    tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
+        ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
+        t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
+        t->d_status);
+  cudaError_t e = cudaGetLastError();
+  if (owned_rows) cudaFreeAsync(owned_rows, st);
+  if (e != cudaSuccess) return cuda_fail(e, "tc_kernel launch", __FILE__, __LINE__);
+  return RESET_OK;
+}
+
+static reset_status sss_common(const reset_table* t, const int32_t* d_off,
+                               const int32_t* d_elems, const int32_t* d_pa,
+                               const int32_t* d_pb, int64_t np, bool float_rule,
+                               int32_t num, int32_t den, float thr,
+                               uint8_t* d_flags, int32_t* d_inter,
+                               reset_stream_t stream) {
+  if (!t) return arg_fail("NULL table");
+  if (np < 0) return arg_fail("negative pair count");
+  if (np == 0) return RESET_OK;
+  if (!d_elems || !d_pa || !d_pb || !d_flags) return arg_fail("NULL pointer");
+  if (!float_rule && (den <= 0 || num < 0)) return arg_fail("threshold num/den");
+  cudaStream_t st = as_stream(stream);
+  DescScope ds;
+  RST_CHECK(resolve_desc(t, d_off, st, &ds));
+#define SSS_LAUNCH(H, F)                                                     \
+  do {                                                                       \
+    const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
+                                 persistent_grid((const void*)sss_kernel<H, F>)); \
+    sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(                           \
+        ds.desc, t->n, d_elems, d_pa, d_pb, np, t->d_table, t->bucket_num,   \
+        t->bucket, t->lg_max, num, den, thr, d_flags, d_inter, t->d_status); \
+  } while (0)
+  if (t->hier) {
+    if (float_rule) SSS_LAUNCH(true, true); else SSS_LAUNCH(true, false);
+  } else {
+    if (float_rule) SSS_LAUNCH(false, true); else SSS_LAUNCH(false, false);
+  }
+#undef SSS_LAUNCH
+  RST_CUDA(cudaGetLastError());
+  return RESET_OK;
+}
+
+reset_status reset_sss(const reset_table* t, const int32_t* d_off,
+                       const int32_t* d_elems, const int32_t* d_pair_a,
+                       const int32_t* d_pair_b, int64_t npairs, int32_t num,
+                       int32_t den, uint8_t* d_flags, int32_t* d_inter,
+                       reset_stream_t stream) {
+  return sss_common(t, d_off, d_elems, d_pair_a, d_pair_b, npairs, false, num,
+                    den, 0.f, d_flags, d_inter, stream);
+}
+
+reset_status reset_sss_float(const reset_table* t, const int32_t* d_off,
+                             const int32_t* d_elems, const int32_t* d_pair_a,
+                             const int32_t* d_pair_b, int64_t npairs,
+                             float thr, uint8_t* d_flags, int32_t* d_inter,
+                             reset_stream_t stream) {
+  return sss_common(t, d_off, d_elems, d_pair_a, d_pair_b, npairs, true, 0, 1,
+                    thr, d_flags, d_inter, stream);
+}
+
+reset_status reset_intersect_count(const int32_t* d_a, int64_t na,
+                                   const int32_t* d_b, int64_t nb,
+                                   const reset_params* params,
+                                   int64_t* d_count, reset_stream_t stream) {
+  if (!d_count) return arg_fail("NULL count");
+  if (na < 0 || nb < 0 || nb > INT32_MAX) return arg_fail("sizes out of range");
+  if ((na > 0 && !d_a) || (nb > 0 && !d_b)) return arg_fail("NULL set");
+  cudaStream_t st = as_stream(stream);
+  RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int64_t), st));
+  if (na == 0 || nb == 0) return RESET_OK;
+  int32_t* d_offb = nullptr;
+  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_offb), 2 * sizeof(int32_t), st));
+  const int32_t h_offb[2] = {0, (int32_t)nb};
+  RST_CUDA(cudaMemcpyAsync(d_offb, h_offb, sizeof(h_offb), cudaMemcpyHostToDevice, st));
+  reset_table* t = nullptr;
+  reset_status s = reset_table_build(d_offb, d_b, 1, nb, params, 0, nullptr, &t, stream);
+  if (s != RESET_OK) {
+    cudaFreeAsync(d_offb, st);
+    return s;
+  }
+  const int lg = t->lg_max;
+  const int64_t g = clamp_grid((na + kThreads - 1) / kThreads,
+                               persistent_grid((const void*)pair_probe_kernel));
+  pair_probe_kernel<<<(int)g, kThreads, 0, st>>>(
+      d_a, na, t->d_table, lg, t->bucket_num, t->bucket,
+      reinterpret_cast<unsigned long long*>(d_count), t->d_status);
+  cudaError_t e = cudaGetLastError();
+  reset_status cs = reset_table_check(t, stream);  // synchronises `stream`
+  cudaFree(d_offb);
+  reset_table_free(t);
+  if (e != cudaSuccess) return cuda_fail(e, "pair_probe_kernel", __FILE__, __LINE__);
+  return cs;
+}
+
+reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
+                      const int32_t* d_docs, const int32_t* d_query,
+                      const int32_t* d_qoff, int32_t nq,
+                      const int64_t* d_res_off, int32_t* d_res,
+                      int32_t* d_cnt, reset_stream_t stream) {
+  if (!t) return arg_fail("NULL table");
+  if (nq < 0) return arg_fail("negative query count");
+  if (nq == 0) return RESET_OK;
+  if (!d_docs || !d_query || !d_qoff || !d_res_off || !d_res || !d_cnt)
+    return arg_fail("NULL pointer");
+  cudaStream_t st = as_stream(stream);
+  DescScope ds;
+  RST_CHECK(resolve_desc(t, d_toff, st, &ds));
+  int64_t* d_sl = nullptr;
+  int64_t* d_tot = nullptr;
+  int32_t* d_slc = nullptr;
+  void* d_tmp = nullptr;
+  reset_status rs = RESET_OK;
+  auto cleanup = [&]() {
+    if (d_sl) cudaFreeAsync(d_sl, st);
+    if (d_tot) cudaFreeAsync(d_tot, st);
+    if (d_slc) cudaFreeAsync(d_slc, st);
+    if (d_tmp) cudaFreeAsync(d_tmp, st);
+  };
+#define IR_CUDA(call)                                                       \
+  do {                                                                      \
+    cudaError_t _e = (call);                                                \
+    if (_e != cudaSuccess) {                                                \
+      rs = cuda_fail(_e, #call, __FILE__, __LINE__);                        \
+      cleanup();                                                            \
+      return rs;                                                            \
+    }                                                                       \
+  } while (0)
+  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_sl), sizeof(int64_t) * (nq + 1), st));
+  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_tot), sizeof(int64_t) * 2, st));
+  ir_plan_kernel<<<(int)clamp_grid((nq + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      ds.desc, t->n, d_query, d_qoff, nq, d_sl, t->d_status);
+  IR_CUDA(cudaGetLastError());
+  // keep the last count, then scan in place
+  IR_CUDA(cudaMemcpyAsync(d_tot + 1, d_sl + (nq - 1), sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+  size_t tb = 0;
+  IR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sl, d_sl, nq, st));
+  IR_CUDA(cudaMallocAsync(&d_tmp, tb, st));
+  IR_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_sl, d_sl, nq, st));
+  ir_total_kernel<<<1, 1, 0, st>>>(d_tot + 1, d_sl, nq, d_tot);
+  IR_CUDA(cudaGetLastError());
+  int64_t total = 0;
+  IR_CUDA(cudaMemcpyAsync(&total, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  IR_CUDA(cudaStreamSynchronize(st));
+  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_slc), sizeof(int32_t) * (total > 0 ? total : 1), st));
+  if (total > 0) {
+#define IR_LAUNCH(H)                                                           \
+    do {                                                                       \
+      const int64_t g = clamp_grid((total + kWarps - 1) / kWarps,              \
+                                   persistent_grid((const void*)ir_slice_kernel<H>)); \
+      ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
+          ds.desc, t->n, d_docs, d_query, d_qoff, nq, d_sl, d_res_off, d_res,  \
+          d_slc, t->d_table, t->bucket_num, t->bucket, t->lg_max, t->d_status); \
+    } while (0)
+    if (t->hier) IR_LAUNCH(true); else IR_LAUNCH(false);
+#undef IR_LAUNCH
+    IR_CUDA(cudaGetLastError());
+  }
+  ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8), kThreads, 0, st>>>(
+      d_sl, nq, d_res_off, d_res, d_slc, d_cnt);
+  IR_CUDA(cudaGetLastError());
+#undef IR_CUDA
+  cleanup();
+  return RESET_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+"""C-ABI boundary checks that need no GPU: the library loads, and exports
+every entry point include/reset.h declares, with bindings for each."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "reset.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set(re.findall(r"\b(reset_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ["reset_table_build", "reset_tc_count", "reset_sss", "reset_ir",
+                 "reset_intersect_count", "reset_csr_hash_order", "reset_table_free"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(libreset):
+    for name in declared_functions():
+        assert hasattr(libreset, name), f"libreset.so does not export {name}"
+
+
+def test_python_binding_covers_header(libreset):
+    from reset_b200 import _lib
+    assert set(declared_functions()) == set(_lib.SIGNATURES)
+
+
+def test_status_strings_and_version(libreset):
+    assert libreset.reset_abi_version() == 1
+    assert libreset.reset_status_string(0) == b"RESET_OK"
+    assert libreset.reset_status_string(4) == b"RESET_ERR_TABLE_FULL"
+
+
+def test_params_default(libreset):
+    from reset_b200 import _lib
+    p = _lib.Params()
+    libreset.reset_params_default(ctypes.byref(p))
+    assert abs(p.alpha - 0.2) < 1e-7 and p.bucket == 5
+
+
+def test_build_rejects_bad_arguments_without_touching_the_gpu(libreset):
+    # Argument validation happens on the host before any CUDA call.
+    from reset_b200 import _lib
+    p = _lib.Params()
+    libreset.reset_params_default(ctypes.byref(p))
+    out = ctypes.c_void_p()
+    st = libreset.reset_table_build(None, None, 4, 0, ctypes.byref(p), 1, None,
+                                    ctypes.byref(out), None)
+    assert st == 3  # RESET_ERR_ARG: NULL offsets
+    p.alpha = 1.5
+    st = libreset.reset_table_build(ctypes.c_void_p(16), None, 0, 0, ctypes.byref(p), 1,
+                                    None, ctypes.byref(out), None)
+    assert st == 3 and b"alpha" in libreset.reset_last_error_string()
+    p.alpha = 0.2
+    p.bucket = 0
+    st = libreset.reset_table_build(ctypes.c_void_p(16), None, 0, 0, ctypes.byref(p), 1,
+                                    None, ctypes.byref(out), None)
+    assert st == 3
+
+
+def test_no_oracle_in_product():
+    """The product package never imports or links the oracle."""
+    pkg = os.path.join(ROOT, "reset_b200")
+    for dp, _, fs in os.walk(pkg):
+        for f in fs:
+            if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
+                txt = open(os.path.join(dp, f)).read()
+                assert "import oracle" not in txt and "liboracle" not in txt, f

@@ -1,0 +1,268 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Integer work, so every comparison is exact: generated graphs, table layout
+(byte for byte), hash-ordered rows, triangle counts, set-similarity flags and
+intersection sizes, retrieval result lists and raw intersection counts.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def R(cuda, libreset):
+    from reset_b200 import api
+    return api
+
+
+def dev(x, torch):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+# ------------------------------------------------------------- generator --
+
+@pytest.mark.parametrize("scale,oriented", [(6, True), (10, True), (12, False), (16, True)])
+def test_gen_rmat_matches_oracle(R, cuda, oracle_mod, scale, oriented):
+    seed = 0x5EED0000 + scale
+    off, cols = R.gen_rmat(scale, 16, seed, oriented=oriented)
+    o_off, o_cols = oracle_mod.rmat_graph(scale, 16, seed, oriented=oriented)
+    assert np.array_equal(host(off), o_off)
+    assert np.array_equal(host(cols), o_cols)
+
+
+# ----------------------------------------------------------- table build --
+
+def _synthetic_csr(rng, sizes, universe):
+    off = np.zeros(len(sizes) + 1, np.int32)
+    off[1:] = np.cumsum(sizes)
+    rows = [np.sort(rng.choice(universe, size=s, replace=False)) if s else np.zeros(0, np.int64)
+            for s in sizes]
+    elems = np.concatenate(rows).astype(np.int32) if off[-1] else np.zeros(0, np.int32)
+    return off, elems
+
+
+def _check_table(R, cuda, O, off, elems, alpha, bucket, hier):
+    t = R.Table(dev(off, cuda), dev(elems, cuda), alpha=alpha, bucket=bucket,
+                hierarchical=hier, hash_order=True)
+    t.check()
+    ot = O.Table(off, elems, alpha=alpha, bucket=bucket, hier=hier)
+    slots, ln, o64 = t.tensors()
+    assert t.bucket_num == ot.bucket_num and t.max_len == ot.max_len
+    assert np.array_equal(host(ln), ot.len)
+    assert np.array_equal(host(o64), ot.off64)
+    assert np.array_equal(host(slots), ot.table), "table layout differs from CSR-order insertion"
+    assert np.array_equal(host(t.hash_order), ot.hash_order())
+    assert np.array_equal(host(t.csr_hash_order()), ot.hash_order())
+    return t, ot
+
+
+@pytest.mark.parametrize("hier", [True, False])
+@pytest.mark.parametrize("alpha,bucket", [(0.2, 5), (0.5, 3), (1.0, 1), (0.1, 9), (0.25, 4)])
+def test_table_layout_rmat(R, cuda, oracle_mod, hier, alpha, bucket):
+    off, cols = oracle_mod.rmat_graph(12, 16, 0x5EED0012, oriented=False)
+    _check_table(R, cuda, oracle_mod, off, cols, alpha, bucket, hier)
+
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_table_layout_ragged_sizes(R, cuda, oracle_mod, hier):
+    """Empty sets, 1-element sets, the thread/warp boundary (8/9), exact
+    powers of two (the strict next-power quirk), tile-sized and big sets,
+    and one set whose fill counts do not fit shared memory."""
+    rng = np.random.default_rng(5)
+    sizes = [0, 1, 0, 5, 8, 9, 16, 31, 32, 33, 100, 0, 1000, 1023, 1024, 1025, 4000,
+             70000, 3, 0, 2]
+    off, elems = _synthetic_csr(rng, sizes, 1 << 22)
+    _check_table(R, cuda, oracle_mod, off, elems, 0.2, 5, hier)
+
+
+def test_table_layout_collisions(R, cuda, oracle_mod):
+    """Keys crowded into few buckets: bucket overflow, spill chains and the
+    wrap-around from the last bucket to bucket 0."""
+    rng = np.random.default_rng(9)
+    sizes = [40, 200, 7, 64, 500]
+    off = np.zeros(len(sizes) + 1, np.int32)
+    off[1:] = np.cumsum(sizes)
+    parts = []
+    for s in sizes:
+        # multiples of a large power of two all share a normal-hash bucket;
+        # values near the top of the id range crowd the last hierarchical bucket
+        base = rng.choice(4096, size=s, replace=False).astype(np.int64)
+        parts.append(np.where(np.arange(s) % 2 == 0, base * 1024, (1 << 30) - 1 - base))
+    elems = np.concatenate(parts).astype(np.int32)
+    for hier in (True, False):
+        for alpha, bucket in [(0.2, 5), (1.0, 2), (1.0, 1)]:
+            _check_table(R, cuda, oracle_mod, off, elems, alpha, bucket, hier)
+
+
+def test_table_empty_inputs(R, cuda, oracle_mod):
+    off = np.zeros(4, np.int32)
+    elems = np.zeros(0, np.int32)
+    _check_table(R, cuda, oracle_mod, off, elems, 0.2, 5, True)
+
+
+def test_table_duplicates_inserted_twice(R, cuda, oracle_mod):
+    # hashtable.cu inserts duplicates as separate slots (no dedupe)
+    off = np.array([0, 6, 6, 9], np.int32)
+    elems = np.array([3, 3, 3, 7, 7, 11, 2, 2, 2], np.int32)
+    _check_table(R, cuda, oracle_mod, off, elems, 0.2, 5, True)
+    _check_table(R, cuda, oracle_mod, off, elems, 1.0, 1, False)
+
+
+# -------------------------------------------------------------------- TC --
+
+@pytest.mark.parametrize("scale", [8, 12, 16])
+@pytest.mark.parametrize("hier", [True, False])
+def test_tc_count_matches_oracle(R, cuda, oracle_mod, scale, hier):
+    off, cols = oracle_mod.rmat_graph(scale, 16, 0x5EED0000 + scale, oriented=True)
+    want = oracle_mod.tc_merge(off, cols)
+    doff, dcols = dev(off, cuda), dev(cols, cuda)
+    t = R.Table(doff, dcols, hierarchical=hier, hash_order=True)
+    assert R.tc_count(t, doff, dcols) == want
+    assert R.tc_count(t, doff, t.hash_order) == want
+    # same offsets in a different buffer: descriptors are rebuilt
+    assert R.tc_count(t, doff.clone(), t.hash_order) == want
+    t.check()
+    ot = oracle_mod.Table(off, cols, hier=hier)
+    assert oracle_mod.tc_hash(ot, ot.hash_order()) == want
+
+
+def test_tc_params_and_generator(R, cuda, oracle_mod):
+    off, cols = R.gen_rmat(14, 16, 0xABCDEF, oriented=True)
+    o_off, o_cols = host(off), host(cols)
+    want = oracle_mod.tc_merge(o_off, o_cols)
+    for alpha, bucket in [(0.2, 5), (0.5, 2), (1.0, 1)]:
+        for hier in (True, False):
+            t = R.Table(off, cols, alpha=alpha, bucket=bucket, hierarchical=hier, hash_order=True)
+            assert R.tc_count(t, off, t.hash_order) == want
+
+
+def test_tc_empty_graph(R, cuda):
+    off = cuda.zeros(9, dtype=cuda.int32, device="cuda")
+    cols = cuda.zeros(0, dtype=cuda.int32, device="cuda")
+    t = R.Table(off, cols)
+    assert R.tc_count(t, off, cols) == 0
+
+
+# ------------------------------------------------------------------- SSS --
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_sss_graph_pairs(R, cuda, oracle_mod, hier):
+    """Reference SSS setting: pairs are the CSR entries (sss.cu:104-105)."""
+    off, cols = oracle_mod.rmat_graph(11, 16, 0x5EED0111, oriented=False)
+    n = off.size - 1
+    pa = np.repeat(np.arange(n, dtype=np.int32), np.diff(off))
+    pb = cols
+    doff, dcols, dpa, dpb = (dev(x, cuda) for x in (off, cols, pa, pb))
+    t = R.Table(doff, dcols, hierarchical=hier)
+    ot = oracle_mod.Table(off, cols, hier=hier)
+    for num, den in [(7, 10), (1, 4), (0, 1), (1, 1)]:
+        f, i = R.sss(t, doff, dcols, dpa, dpb, num, den)
+        of, oi = oracle_mod.sss(ot, pa, pb, mode=1, num=num, den=den)
+        assert np.array_equal(host(i), oi)
+        assert np.array_equal(host(f), of)
+    for thr in [0.25, 0.7, 0.5, 1.0 / 3.0]:
+        f, i = R.sss_float(t, doff, dcols, dpa, dpb, thr)
+        of, oi = oracle_mod.sss(ot, pa, pb, mode=0, thr=thr)
+        assert np.array_equal(host(f), of)
+
+
+def test_sss_random_pairs_and_empty_sets(R, cuda, oracle_mod):
+    rng = np.random.default_rng(3)
+    sizes = rng.integers(0, 300, size=500)
+    sizes[::17] = 0
+    off, elems = _synthetic_csr(rng, sizes, 2000)
+    P = 20000
+    pa = rng.integers(0, 500, size=P).astype(np.int32)
+    pb = rng.integers(0, 500, size=P).astype(np.int32)
+    pb[:50] = pa[:50]  # identical sets: Jaccard 1 (or U = 0 for empty sets)
+    doff, de, dpa, dpb = (dev(x, cuda) for x in (off, elems, pa, pb))
+    for hier in (True, False):
+        t = R.Table(doff, de, hierarchical=hier, hash_order=True)
+        ot = oracle_mod.Table(off, elems, hier=hier)
+        f, i = R.sss(t, doff, t.hash_order, dpa, dpb, 7, 10)
+        of, oi = oracle_mod.sss(ot, pa, pb, mode=1, num=7, den=10)
+        assert np.array_equal(host(i), oi) and np.array_equal(host(f), of)
+        f, i = R.sss_float(t, doff, de, dpa, dpb, 0.7)
+        of, _ = oracle_mod.sss(ot, pa, pb, mode=0, thr=0.7)
+        assert np.array_equal(host(f), of)
+
+
+# -------------------------------------------------------------------- IR --
+
+def _ir_index(rng, nterms, ndocs, npost, nq, empty_every=0):
+    w = 1.0 / np.arange(1, nterms + 1) ** 1.1
+    df = np.minimum(np.maximum(1, np.round(w / w.sum() * npost)), ndocs).astype(np.int64)
+    df[::11] = 0  # terms with no postings
+    lists = [np.sort(rng.choice(ndocs, size=int(k), replace=False)).astype(np.int32) for k in df]
+    toff = np.zeros(nterms + 1, np.int32)
+    toff[1:] = np.cumsum([l.size for l in lists])
+    docs = np.concatenate(lists).astype(np.int32)
+    p = (df + 1) / (df + 1).sum()
+    q, qoff = [], [0]
+    for i in range(nq):
+        k = 0 if (empty_every and i % empty_every == 0) else int(rng.integers(1, 7))
+        ts = np.unique(rng.choice(nterms, size=k, p=p)) if k else []
+        ts = sorted(list(ts), key=lambda t: (int(df[t]), int(t)))
+        q.extend(ts)
+        qoff.append(len(q))
+    return toff, docs, np.array(q, np.int32), np.array(qoff, np.int32)
+
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_ir_matches_oracle(R, cuda, oracle_mod, hier):
+    rng = np.random.default_rng(21)
+    toff, docs, query, qoff = _ir_index(rng, 400, 60000, 300000, 700, empty_every=50)
+    dt, dd, dq, dqo = (dev(x, cuda) for x in (toff, docs, query, qoff))
+    t = R.Table(dt, dd, hierarchical=hier, hash_order=True)
+    ot = oracle_mod.Table(toff, docs, hier=hier)
+    for dsrc, osrc in [(dd, docs), (t.hash_order, ot.hash_order())]:
+        roff, res, cnt = R.ir(t, dt, dsrc, dq, dqo)
+        oroff, ores, ocnt = oracle_mod.ir(ot, query, qoff, docs=osrc)
+        assert np.array_equal(host(roff), oroff)
+        assert np.array_equal(host(cnt), ocnt)
+        hr = host(res)
+        for qi in range(qoff.size - 1):
+            a, c = oroff[qi], ocnt[qi]
+            assert np.array_equal(hr[a:a + c], ores[a:a + c]), f"query {qi}"
+    t.check()
+
+
+def test_ir_long_first_lists(R, cuda, oracle_mod):
+    """First-term lists longer than one work slice (several slices per query)."""
+    rng = np.random.default_rng(4)
+    ndocs = 200000
+    lists = [np.sort(rng.choice(ndocs, size=s, replace=False)).astype(np.int32)
+             for s in [50000, 60000, 9000, 120000, 7]]
+    toff = np.zeros(len(lists) + 1, np.int32)
+    toff[1:] = np.cumsum([l.size for l in lists])
+    docs = np.concatenate(lists)
+    query = np.array([0, 1, 3, 1, 3, 0, 1, 2, 3, 1], np.int32)
+    qoff = np.array([0, 3, 5, 7, 9, 10], np.int32)
+    dt, dd, dq, dqo = (dev(x, cuda) for x in (toff, docs, query, qoff))
+    t = R.Table(dt, dd)
+    ot = oracle_mod.Table(toff, docs)
+    roff, res, cnt = R.ir(t, dt, dd, dq, dqo)
+    oroff, ores, ocnt = oracle_mod.ir(ot, query, qoff)
+    assert np.array_equal(host(cnt), ocnt)
+    hr = host(res)
+    for qi in range(qoff.size - 1):
+        a, c = oroff[qi], ocnt[qi]
+        assert np.array_equal(hr[a:a + c], ores[a:a + c])
+
+
+# -------------------------------------------------------------- raw pair --
+
+@pytest.mark.parametrize("na,nb,universe", [
+    (1, 1, 4), (16, 100, 64), (1000, 3000, 6000), (4096, 4096, 1 << 14),
+    (1 << 20, 1 << 16, 1 << 22), (1 << 16, 1 << 20, 1 << 21), (0, 10, 10), (10, 0, 10)])
+def test_intersect_count(R, cuda, oracle_mod, na, nb, universe):
+    rng = np.random.default_rng(na * 7 + nb)
+    a = rng.integers(0, universe, size=na).astype(np.int32)
+    b = rng.integers(0, universe, size=nb).astype(np.int32)
+    got = R.intersect_count(dev(a, cuda), dev(b, cuda))
+    assert got == oracle_mod.pair_count(a, b)
