@@ -191,6 +191,9 @@ reset_status reset_free(void *d_ptr);
 const char *reset_last_error_string(void);
 const char *reset_status_string(int32_t status);
 int32_t reset_abi_version(void);
+/* Number of launches of libreset's own kernels in this process so far
+ * (library routines it calls, such as CUB scans, are not counted). */
+int64_t reset_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,7 @@ SIGNATURES = {
     "reset_last_error_string": (C.c_char_p, []),
     "reset_status_string": (C.c_char_p, [I32]),
     "reset_abi_version": (I32, []),
+    "reset_kernel_launches": (I64, []),
 }
 
 _lib = None

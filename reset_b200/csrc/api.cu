@@ -1,4 +1,5 @@
 // Error reporting, version and small helpers of the C ABI.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -8,6 +9,9 @@
 namespace rst {
 
 static thread_local char g_err[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -62,6 +66,10 @@ const char* reset_status_string(int32_t s) {
 }
 
 int32_t reset_abi_version(void) { return RESET_ABI_VERSION; }
+
+int64_t reset_kernel_launches(void) {
+  return rst::g_launches.load(std::memory_order_relaxed);
+}
 
 void reset_params_default(reset_params* p) {
   if (!p) return;

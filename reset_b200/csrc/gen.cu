@@ -138,7 +138,7 @@ extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
   GEN_CUDA(cudaMalloc(&k0, sizeof(uint64_t) * nk));
   GEN_CUDA(cudaMalloc(&k1, sizeof(uint64_t) * nk));
   GEN_CUDA(cudaMalloc(&d_cnt, sizeof(int64_t) * 2));
-  rmat_kernel<<<gen_grid(ne), 256, 0, st>>>(seed, scale, ne, ta, tb, tc, k0);
+  note_launch(); rmat_kernel<<<gen_grid(ne), 256, 0, st>>>(seed, scale, ne, ta, tb, tc, k0);
   GEN_CUDA(cudaGetLastError());
   cub::DoubleBuffer<uint64_t> db(k0, k1);
   size_t tb_sort = 0, tb_uniq = 0, tb_flag = 0, tb_scan = 0;
@@ -173,8 +173,8 @@ extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
   GEN_CUDA(cudaMemsetAsync(deg, 0, sizeof(int32_t) * n, st));
   GEN_CUDA(cudaMemsetAsync(outdeg, 0, sizeof(int32_t) * (n + 1), st));
   if (nu > 0) {
-    degree_kernel<<<gen_grid(nu), 256, 0, st>>>(other, nu, deg);
-    orient_kernel<<<gen_grid(nu), 256, 0, st>>>(other, nu, deg, oriented, keep, outdeg);
+    note_launch(); degree_kernel<<<gen_grid(nu), 256, 0, st>>>(other, nu, deg);
+    note_launch(); orient_kernel<<<gen_grid(nu), 256, 0, st>>>(other, nu, deg, oriented, keep, outdeg);
     GEN_CUDA(cudaGetLastError());
     GEN_CUDA(cub::DeviceSelect::Flagged(tmp, tb_flag, other, keep, sorted, d_cnt, (int)nu, st));
   } else {
@@ -189,7 +189,7 @@ extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
   GEN_CUDA(cudaMalloc(&cols, sizeof(int32_t) * (m > 0 ? m : 1)));
   GEN_CUDA(cudaMemcpyAsync(off, outdeg, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice, st));
   if (m > 0) {
-    cols_kernel<<<gen_grid(m), 256, 0, st>>>(sorted, m, cols);
+    note_launch(); cols_kernel<<<gen_grid(m), 256, 0, st>>>(sorted, m, cols);
     GEN_CUDA(cudaGetLastError());
   }
 #undef GEN_CUDA

@@ -438,16 +438,17 @@ reset_status reset_tc_count(const reset_table* t, const int32_t* d_off,
   }
   const void* k = t->hier ? (const void*)tc_kernel<true> : (const void*)tc_kernel<false>;
   const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps, persistent_grid(k));
-  if (t->hier)
-    tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
+  if (t->hier) {
+    note_launch(); tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
         ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
         t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
         t->d_status);
-  else
-    tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
+  } else {
+    note_launch(); tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
         ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
         t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
         t->d_status);
+  }
   cudaError_t e = cudaGetLastError();
   if (owned_rows) cudaFreeAsync(owned_rows, st);
   if (e != cudaSuccess) return cuda_fail(e, "tc_kernel launch", __FILE__, __LINE__);
@@ -472,7 +473,7 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   do {                                                                       \
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
                                  persistent_grid((const void*)sss_kernel<H, F>)); \
-    sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(                           \
+    note_launch(); sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(                           \
         ds.desc, t->n, d_elems, d_pa, d_pb, np, t->d_table, t->bucket_num,   \
         t->bucket, t->lg_max, num, den, thr, d_flags, d_inter, t->d_status); \
   } while (0)
@@ -527,7 +528,7 @@ reset_status reset_intersect_count(const int32_t* d_a, int64_t na,
   const int lg = t->lg_max;
   const int64_t g = clamp_grid((na + kThreads - 1) / kThreads,
                                persistent_grid((const void*)pair_probe_kernel));
-  pair_probe_kernel<<<(int)g, kThreads, 0, st>>>(
+  note_launch(); pair_probe_kernel<<<(int)g, kThreads, 0, st>>>(
       d_a, na, t->d_table, lg, t->bucket_num, t->bucket,
       reinterpret_cast<unsigned long long*>(d_count), t->d_status);
   cudaError_t e = cudaGetLastError();
@@ -573,7 +574,7 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   } while (0)
   IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_sl), sizeof(int64_t) * (nq + 1), st));
   IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_tot), sizeof(int64_t) * 2, st));
-  ir_plan_kernel<<<(int)clamp_grid((nq + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+  note_launch(); ir_plan_kernel<<<(int)clamp_grid((nq + 255) / 256, sm_count() * 8), 256, 0, st>>>(
       ds.desc, t->n, d_query, d_qoff, nq, d_sl, t->d_status);
   IR_CUDA(cudaGetLastError());
   // keep the last count, then scan in place
@@ -582,7 +583,7 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   IR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sl, d_sl, nq, st));
   IR_CUDA(cudaMallocAsync(&d_tmp, tb, st));
   IR_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_sl, d_sl, nq, st));
-  ir_total_kernel<<<1, 1, 0, st>>>(d_tot + 1, d_sl, nq, d_tot);
+  note_launch(); ir_total_kernel<<<1, 1, 0, st>>>(d_tot + 1, d_sl, nq, d_tot);
   IR_CUDA(cudaGetLastError());
   int64_t total = 0;
   IR_CUDA(cudaMemcpyAsync(&total, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -593,7 +594,7 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
     do {                                                                       \
       const int64_t g = clamp_grid((total + kWarps - 1) / kWarps,              \
                                    persistent_grid((const void*)ir_slice_kernel<H>)); \
-      ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
+      note_launch(); ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
           ds.desc, t->n, d_docs, d_query, d_qoff, nq, d_sl, d_res_off, d_res,  \
           d_slc, t->d_table, t->bucket_num, t->bucket, t->lg_max, t->d_status); \
     } while (0)
@@ -601,7 +602,7 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
 #undef IR_LAUNCH
     IR_CUDA(cudaGetLastError());
   }
-  ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8), kThreads, 0, st>>>(
+  note_launch(); ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8), kThreads, 0, st>>>(
       d_sl, nq, d_res_off, d_res, d_slc, d_cnt);
   IR_CUDA(cudaGetLastError());
 #undef IR_CUDA

@@ -496,7 +496,7 @@ reset_status make_chunk_rows(const int32_t* d_off, int32_t n, int64_t m,
   RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d_rows_out),
                            sizeof(int32_t) * (nc > 0 ? nc : 1), st));
   RST_CUDA(cudaMemsetAsync(*d_rows_out, 0, sizeof(int32_t) * (nc > 0 ? nc : 1), st));
-  layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
+  note_launch(); layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
       d_off, nullptr, nullptr, n, nullptr, *d_rows_out, nullptr, 1, 0);
   RST_CUDA(cudaGetLastError());
   return RESET_OK;
@@ -521,7 +521,7 @@ reset_status make_desc(const reset_table* t, const int32_t* d_off,
                        int4** d_desc_out, cudaStream_t st) {
   RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d_desc_out),
                            sizeof(int4) * (t->n > 0 ? t->n : 1), st));
-  redesc_kernel<<<grid_for(t->n, 256), 256, 0, st>>>(d_off, t->d_desc, t->n,
+  note_launch(); redesc_kernel<<<grid_for(t->n, 256), 256, 0, st>>>(d_off, t->d_desc, t->n,
                                                      *d_desc_out);
   RST_CUDA(cudaGetLastError());
   return RESET_OK;
@@ -553,7 +553,7 @@ reset_status launch_builds(const reset_table* t, const int32_t* d_off,
     RST_CUDA(cudaFuncSetAttribute(tile_build_kernel<HIER>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)g.smem));
-    tile_build_kernel<HIER><<<n_tiles, kThreads, g.smem, st>>>(
+    note_launch(); tile_build_kernel<HIER><<<n_tiles, kThreads, g.smem, st>>>(
         d_off, d_elems, t->d_len, t->d_off64, d_tile_first, t->bucket_num,
         t->bucket, t->lg_max, g.R_max, g.LT, t->d_table, d_hash_out,
         t->d_status);
@@ -564,7 +564,7 @@ reset_status launch_builds(const reset_table* t, const int32_t* d_off,
     RST_CUDA(cudaFuncSetAttribute(big_build_kernel<HIER>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm));
-    big_build_kernel<HIER><<<n_big, kThreads, sm, st>>>(
+    note_launch(); big_build_kernel<HIER><<<n_big, kThreads, sm, st>>>(
         d_off, d_elems, t->d_len, t->d_off64, d_big, t->bucket_num, t->bucket,
         t->lg_max, t->d_table, d_hash_out, t->d_status);
     RST_CUDA(cudaGetLastError());
@@ -636,7 +636,7 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   BUILD_CUDA(cudaMalloc(&d_big, sizeof(int32_t) * (n > 0 ? n : 1)));
 
   if (n > 0) {
-    meta_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_off, n, p.alpha, p.bucket,
+    note_launch(); meta_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_off, n, p.alpha, p.bucket,
                                                    g.LT, t->d_len, t->d_off64,
                                                    d_info, d_big, t->d_status);
     BUILD_CUDA(cudaGetLastError());
@@ -647,7 +647,7 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
     BUILD_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, t->d_off64,
                                              t->d_off64, n, st));
   }
-  finalize_kernel<<<1, 1, 0, st>>>(t->d_len, t->d_off64, n, d_bn);
+  note_launch(); finalize_kernel<<<1, 1, 0, st>>>(t->d_len, t->d_off64, n, d_bn);
   BUILD_CUDA(cudaGetLastError());
   int32_t info[4];
   int64_t bn = 0;
@@ -671,7 +671,7 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   const int32_t n_tiles = (int32_t)n_tiles64;
   BUILD_CUDA(cudaMalloc(&d_tile_first, sizeof(int32_t) * (n_tiles + 1)));
   if (n > 0) {
-    layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
+    note_launch(); layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
         d_off, t->d_off64, t->d_len, n, t->d_desc, t->d_chunk_row,
         d_tile_first, g.T, n_tiles);
     BUILD_CUDA(cudaGetLastError());
@@ -745,7 +745,7 @@ reset_status reset_csr_hash_order(const reset_table* t, const int32_t* d_off,
     return arg_fail("NULL table, offsets or output");
   if (t->n == 0) return RESET_OK;
   cudaStream_t st = as_stream(stream);
-  extract_kernel<<<grid_for((int64_t)t->n * 32, kThreads), kThreads, 0, st>>>(
+  note_launch(); extract_kernel<<<grid_for((int64_t)t->n * 32, kThreads), kThreads, 0, st>>>(
       d_off, t->d_off64, t->n, t->d_table, t->bucket_num, t->bucket,
       d_cols_out);
   RST_CUDA(cudaGetLastError());

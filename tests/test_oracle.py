@@ -1,0 +1,219 @@
+"""The CPU oracle: unit checks of the restated rules, and its pinning against
+golden outputs of the reference's own kernels (tests/golden/*.npz, made by
+tests/golden/make_golden.py from the reference sources compiled unchanged)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+# ------------------------------------------------------------ unit rules --
+
+
+def test_calc_len_rule(oracle_mod):
+    O = oracle_mod
+    # t = (int)(d / 0.2f); L = t / 5; 0 -> 8; strict next power of two; >= 8
+    assert [O.calc_len(d) for d in [0, 1, 2, 7]] == [8, 8, 8, 8]
+    assert O.calc_len(8) == 16      # L = 8 exactly: doubled (hashtable.cu:27-32)
+    assert O.calc_len(15) == 16
+    assert O.calc_len(16) == 32
+    assert O.calc_len(1000) == 1024
+    assert O.calc_len(1024) == 2048
+    assert O.calc_len(10, 0.5, 3) == 8     # t=20, L=6 -> 8
+    assert O.calc_len(100, 0.5, 3) == 128  # t=200, L=66 -> 128
+    assert O.calc_len(64, 1.0, 1) == 128
+
+
+def test_calc_len_float_division_matches_float32(oracle_mod):
+    a = np.float32(0.2)
+    for d in list(range(0, 5000)) + [2 ** 20 + 3, 12345679]:
+        t = int(np.float32(d) / a)
+        L = t // 5
+        want = 8 if L == 0 else max(8, 1 << int(L).bit_length())
+        assert oracle_mod.calc_len(d) == want, d
+
+
+def test_hash_functions(oracle_mod):
+    O = oracle_mod
+    assert O.lib().ro_hash_normal(1234567, 64) == 1234567 & 63
+    # hierarchical: (x & (max-1)) >> (log2 max - log2 len)
+    assert O.lib().ro_hash_hier(0b110101101, 8, 512) == (0b110101101 & 511) >> 6
+    assert O.lib().ro_hash_hier(77, 512, 512) == 77
+
+
+def test_table_is_valid_and_hash_order_is_row_permutation(oracle_mod):
+    O = oracle_mod
+    off, cols = O.rmat_graph(10, 16, 77, oriented=False)
+    for hier in (0, 1):
+        t = O.Table(off, cols, hier=hier)
+        tab = t.table.reshape(t.bucket, t.bucket_num)
+        for u in range(0, off.size - 1, 37):
+            region = tab[:, t.off64[u]:t.off64[u + 1]]
+            got = np.sort(region[region != -1])
+            assert np.array_equal(got, np.sort(cols[off[u]:off[u + 1]]))
+        ho = t.hash_order()
+        for u in range(0, off.size - 1, 41):
+            assert np.array_equal(np.sort(ho[off[u]:off[u + 1]]), np.sort(cols[off[u]:off[u + 1]]))
+
+
+def test_tc_hash_equals_merge(oracle_mod):
+    O = oracle_mod
+    off, cols = O.rmat_graph(11, 16, 99, oriented=True)
+    want = O.tc_merge(off, cols)
+    assert want > 0
+    for hier in (0, 1):
+        for alpha, b in [(0.2, 5), (1.0, 1), (0.5, 3)]:
+            t = O.Table(off, cols, alpha=alpha, bucket=b, hier=hier)
+            assert O.tc_hash(t) == want
+            assert O.tc_hash(t, t.hash_order()) == want
+
+
+def test_sss_rules(oracle_mod):
+    O = oracle_mod
+    # A = {1,2,3,4}, B = {2,3,4,5,6}: I = 3, U = 6
+    off = np.array([0, 4, 9, 9], np.int32)
+    el = np.array([1, 2, 3, 4, 2, 3, 4, 5, 6], np.int32)
+    t = O.Table(off, el)
+    f, i = O.sss(t, [0, 0, 2], [1, 0, 2], mode=1, num=1, den=2)
+    assert list(i) == [3, 4, 0] and list(f) == [1, 1, 0]  # empty pair: U = 0 -> 0
+    f, _ = O.sss(t, [0], [1], mode=1, num=7, den=10)
+    assert list(f) == [0]
+    f, _ = O.sss(t, [0, 2], [1, 2], mode=0, thr=0.5)
+    assert list(f) == [1, 0]  # 0/0 is NaN in the float rule: not similar
+
+
+def test_ir_rule(oracle_mod):
+    O = oracle_mod
+    toff = np.array([0, 3, 8, 10, 10], np.int32)
+    docs = np.array([5, 9, 12, 1, 5, 9, 12, 40, 9, 12], np.int32)
+    t = O.Table(toff, docs)
+    query = np.array([0, 1, 2, 2, 0, 3, 1], np.int32)
+    qoff = np.array([0, 3, 5, 5, 6, 7], np.int32)
+    roff, res, cnt = O.ir(t, query, qoff)
+    assert list(cnt) == [2, 2, 0, 0, 5]
+    assert list(res[roff[0]:roff[0] + 2]) == [9, 12]
+    assert list(res[roff[4]:roff[4] + 5]) == [1, 5, 9, 12, 40]
+
+
+def test_pair_count_multiplicity(oracle_mod):
+    assert oracle_mod.pair_count([1, 1, 2, 7], [1, 2, 2, 3]) == 3
+    assert oracle_mod.pair_count([], [1]) == 0
+
+
+def test_rmat_graph_properties(oracle_mod):
+    off, cols = oracle_mod.rmat_graph(9, 8, 1234, oriented=False)
+    n = off.size - 1
+    src = np.repeat(np.arange(n), np.diff(off))
+    assert np.all(src != cols)                       # no self-loops
+    key = src.astype(np.int64) * n + cols
+    assert np.all(np.diff(key) > 0)                  # sorted, no duplicates
+    sym = set(zip(src.tolist(), cols.tolist()))
+    assert all((v, u) in sym for u, v in sym)        # symmetric
+    o_off, o_cols = oracle_mod.rmat_graph(9, 8, 1234, oriented=True)
+    assert o_cols.size * 2 == cols.size
+    deg = np.diff(off)
+    o_src = np.repeat(np.arange(n), np.diff(o_off))
+    assert np.all((deg[o_src] < deg[o_cols]) | ((deg[o_src] == deg[o_cols]) & (o_src < o_cols)))
+
+
+# ---------------------------------------------------------------- golden --
+
+GOLDEN_CASES = ["tc_s10", "tc_s11_a05_b3", "sss_s9_t025", "sss_s9_t07", "ir_small",
+                "pair_1000_3000", "pair_4096_4096", "pair_17_100"]
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def test_golden_fixtures_present():
+    have = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))}
+    assert set(GOLDEN_CASES) <= have
+
+
+def _regions_equal_as_multisets(O, t, ref_table, off, elems):
+    tab = ref_table.reshape(t.bucket, t.bucket_num)
+    mine = t.table.reshape(t.bucket, t.bucket_num)
+    for u in range(off.size - 1):
+        a, b = t.off64[u], t.off64[u + 1]
+        r = tab[:, a:b]
+        got = np.sort(r[r != -1])
+        assert np.array_equal(got, np.sort(elems[off[u]:off[u + 1]])), u
+        # linear probing fills the same slots whatever the insertion order
+        assert np.array_equal(r != -1, mine[:, a:b] != -1), u
+
+
+@pytest.mark.parametrize("name", ["tc_s10", "tc_s11_a05_b3"])
+def test_oracle_matches_reference_tc(oracle_mod, name):
+    O = oracle_mod
+    g = _load(name)
+    off, cols = g["off"], g["cols"]
+    alpha, b = float(g["alpha"]), int(g["bucket"])
+    max_len, bucket_num, c_norm, c_hier = (int(x) for x in g["ref_meta"])
+    # the inputs are re-creatable from the seed
+    o2, c2 = O.rmat_graph(int(g["scale"]), 16, int(g["seed"]), oriented=True)
+    assert np.array_equal(o2, off) and np.array_equal(c2, cols)
+    want = O.tc_merge(off, cols)
+    assert c_norm == want and c_hier == want
+    for hier, key in [(0, "ref_table_normal"), (1, "ref_table_hier")]:
+        t = O.Table(off, cols, alpha=alpha, bucket=b, hier=hier)
+        assert t.max_len == max_len and t.bucket_num == bucket_num
+        assert np.array_equal(t.len, g["ref_len"]) and np.array_equal(t.off64, g["ref_off64"])
+        assert O.tc_hash(t) == want
+        _regions_equal_as_multisets(O, t, g[key], off, cols)
+        # every key of the reference's own table is found by the probe rule
+        t.table = np.ascontiguousarray(g[key])
+        assert O.tc_hash(t) == want
+        assert O.tc_hash(t, g["ref_cols_hier_sorted"]) == want
+    # the reference's sort keeps every row's multiset, ordered by col % max_len
+    srt = g["ref_cols_hier_sorted"]
+    for u in range(off.size - 1):
+        r = srt[off[u]:off[u + 1]]
+        assert np.array_equal(np.sort(r), np.sort(cols[off[u]:off[u + 1]]))
+        assert np.all(np.diff(r % max_len) >= 0)
+
+
+@pytest.mark.parametrize("name", ["sss_s9_t025", "sss_s9_t07"])
+def test_oracle_matches_reference_sss(oracle_mod, name):
+    O = oracle_mod
+    g = _load(name)
+    off, cols, thr = g["off"], g["cols"], float(g["thr"])
+    n = off.size - 1
+    pa = np.repeat(np.arange(n, dtype=np.int32), np.diff(off))
+    max_len, bucket_num, s_norm, s_hier = (int(x) for x in g["ref_meta"])
+    for hier in (0, 1):
+        t = O.Table(off, cols, hier=hier)
+        assert t.max_len == max_len and t.bucket_num == bucket_num
+        f, _ = O.sss(t, pa, cols, mode=0, thr=thr)
+        if hier == 0:
+            assert np.array_equal(f.astype(np.int32), g["ref_results_normal"])
+        assert int(f.sum()) == s_norm == s_hier
+
+
+def test_oracle_matches_reference_ir(oracle_mod):
+    O = oracle_mod
+    g = _load("ir_small")
+    toff, docs, query, qoff = g["toff"], g["docs"], g["query"], g["qoff"]
+    for hier, suffix in [(0, "normal"), (1, "hier")]:
+        t = O.Table(toff, docs, hier=hier)
+        src = docs if hier == 0 else g["ref_docs_hier_sorted"]
+        roff, res, cnt = O.ir(t, query, qoff, docs=src)
+        assert np.array_equal(roff, g["ref_result_offsets"])
+        assert np.array_equal(cnt, g["ref_count_" + suffix])
+        ref = g["ref_result_" + suffix]
+        for q in range(qoff.size - 1):
+            a, c = roff[q], cnt[q]
+            # exact order: first-term order filtered (ir.cu:131-161)
+            assert np.array_equal(res[a:a + c], ref[a:a + c]), (suffix, q)
+
+
+@pytest.mark.parametrize("name", ["pair_1000_3000", "pair_4096_4096", "pair_17_100"])
+def test_oracle_matches_reference_pair(oracle_mod, name):
+    g = _load(name)
+    a, b = g["a"], g["b"]
+    if a.size > b.size:  # intersection.cu:198-202 probes the smaller set
+        a, b = b, a
+    _, c_norm, c_opt = (int(x) for x in g["ref_meta"])
+    assert c_norm == c_opt == oracle_mod.pair_count(a, b)
