@@ -126,6 +126,17 @@ reset_status reset_tc_count(const reset_table *t, const int32_t *d_off,
                             const int32_t *d_cols, int64_t m,
                             uint64_t *d_count, reset_stream_t stream);
 
+/* reset_tc_count with an explicit method (same count either way):
+ *   0 = default (2);
+ *   1 = edge-flattened: 32 edges per warp, their probes flattened across the
+ *       lanes, both sides read from HBM (the reference's access pattern);
+ *   2 = vertex-staged: each row staged once in shared memory (keys + hash
+ *       set) and reused by all its out-edges. */
+reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
+                               const int32_t *d_cols, int64_t m,
+                               int32_t method, uint64_t *d_count,
+                               reset_stream_t stream);
+
 /* Set-similarity decisions for P explicit pairs (d_pair_a[p], d_pair_b[p])
  * of sets of the table's CSR.  I = |A ∩ B| by probing the smaller set into
  * the larger set's table; U = |A| + |B| - I.
@@ -174,14 +185,20 @@ reset_status reset_intersect_count(const int32_t *d_a, int64_t na,
 
 /* ---- synthetic inputs (stand-ins for the reference's datasets) -------- */
 
+/* Options of reset_gen_rmat. */
+#define RESET_GEN_SYMMETRIC 1 /* full symmetric adjacency instead of oriented */
+#define RESET_GEN_KEEP_IDS 2  /* keep raw R-MAT ids (no relabeling)          */
+
 /* Seeded R-MAT graph on the device: 2^scale vertices, edge_factor*2^scale
- * generated edges; self-loops and duplicates removed, symmetrised.
- * oriented = 1: keep u->v iff (deg u, u) < (deg v, v) (triangle-counting
- * input); oriented = 0: full symmetric adjacency.  Rows sorted ascending.
- * Outputs are allocated with cudaMalloc and owned by the caller (free with
- * reset_free).  Synchronises `stream`. */
+ * generated edges, vertex labels relabeled by a seeded bijection (the
+ * Graph500 convention; RESET_GEN_KEEP_IDS skips it), self-loops and
+ * duplicates removed, symmetrised.  Default: keep u->v iff
+ * (deg u, u) < (deg v, v) (triangle-counting input); RESET_GEN_SYMMETRIC:
+ * full symmetric adjacency.  Rows sorted ascending.  Outputs are allocated
+ * with cudaMalloc and owned by the caller (free with reset_free).
+ * Synchronises `stream`. */
 reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed,
-                            double a, double b, double c, int32_t oriented,
+                            double a, double b, double c, int32_t options,
                             int32_t **d_off_out, int32_t **d_cols_out,
                             int64_t *m_out, reset_stream_t stream);
 reset_status reset_free(void *d_ptr);

@@ -81,6 +81,8 @@ def lib():
         L.ro_ir.restype = None
         L.ro_pair_count.argtypes = [_i32p, C.c_int64, _i32p, C.c_int64]
         L.ro_pair_count.restype = C.c_int64
+        L.ro_relabel.argtypes = [C.c_uint64, C.c_int32, C.c_uint32]
+        L.ro_relabel.restype = C.c_uint32
         L.ro_mix64.argtypes = [C.c_uint64]
         L.ro_mix64.restype = C.c_uint64
         L.ro_rmat_graph.argtypes = [C.c_int32, C.c_int32, C.c_uint64,
@@ -210,9 +212,10 @@ def pair_count(a, b) -> int:
 # ------------------------------------------------------------- generators ---
 
 def rmat_graph(scale, edge_factor=16, seed=0x5EED0016, a=0.57, b=0.19, c=0.19,
-               oriented=True):
+               oriented=True, relabel=True):
     """-> (off int32[n+1], cols int32[m]) (see ro_rmat_graph)."""
-    g = lib().ro_rmat_graph(scale, edge_factor, seed, a, b, c, 0 if oriented else 1)
+    mode = (0 if oriented else 1) | (0 if relabel else 2)
+    g = lib().ro_rmat_graph(scale, edge_factor, seed, a, b, c, mode)
     try:
         n, m = g.contents.n, g.contents.m
         off = np.ctypeslib.as_array(g.contents.off, shape=(n + 1,)).copy()

@@ -428,6 +428,19 @@ void ro_rmat_edge(uint64_t seed, int64_t i, int32_t scale, int32_t ta,
   *pv = (int32_t)v;
 }
 
+uint32_t ro_relabel(uint64_t seed, int32_t scale, uint32_t x) {
+  uint32_t mask = scale >= 32 ? 0xFFFFFFFFu : ((1u << scale) - 1u);
+  int32_t sh = (scale + 1) / 2;
+  for (int r = 0; r < 3; r++) {
+    uint32_t M = (uint32_t)ro_mix64(seed ^ (0x5EC0DE00ull + 2 * r)) | 1u;
+    uint32_t A = (uint32_t)ro_mix64(seed ^ (0x5EC0DE01ull + 2 * r));
+    x = (x * M) & mask;
+    x ^= x >> sh;
+    x = (x + A) & mask;
+  }
+  return x;
+}
+
 static void radix_sort_u64(uint64_t *x, int64_t n) {
   uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(n > 0 ? n : 1));
   int64_t cnt[65536];
@@ -458,6 +471,10 @@ ro_csr *ro_rmat_graph(int32_t scale, int32_t edge_factor, uint64_t seed,
   for (int64_t i = 0; i < ne; i++) {
     int32_t u, v;
     ro_rmat_edge(seed, i, scale, ta, tb, tc, &u, &v);
+    if (!(mode & 2)) {
+      u = (int32_t)ro_relabel(seed, scale, (uint32_t)u);
+      v = (int32_t)ro_relabel(seed, scale, (uint32_t)v);
+    }
     if (u == v) continue; /* self-loops removed */
     keys[k++] = ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
     keys[k++] = ((uint64_t)(uint32_t)v << 32) | (uint32_t)u;
@@ -475,7 +492,7 @@ ro_csr *ro_rmat_graph(int32_t scale, int32_t edge_factor, uint64_t seed,
   for (int64_t i = 0; i < m; i++) {
     int32_t u = (int32_t)(keys[i] >> 32), v = (int32_t)(keys[i] & 0xFFFFFFFFu);
     int keep = 1;
-    if (mode == 0) /* orient low degree -> high degree, ties by id */
+    if ((mode & 1) == 0) /* orient low degree -> high degree, ties by id */
       keep = deg[u] < deg[v] || (deg[u] == deg[v] && u < v);
     if (keep) {
       keys[w++] = keys[i];

@@ -117,6 +117,13 @@ void ro_rmat_thresholds(double a, double b, double c, int32_t *ta,
 void ro_rmat_edge(uint64_t seed, int64_t i, int32_t scale, int32_t ta,
                   int32_t tb, int32_t tc, int32_t *u, int32_t *v);
 
+/* Seeded bijection of [0, 2^scale) used to relabel R-MAT vertices (the
+ * Graph500 Kronecker generator permutes vertex labels the same way, so that
+ * ids carry no trace of the recursive quadrant choice): three rounds of
+ * x = (x * M_r) mod 2^scale; x ^= x >> ceil(scale/2); x = (x + A_r) mod 2^scale,
+ * M_r = mix64(seed ^ (0x5EC0DE00 + 2r)) | 1, A_r = mix64(seed ^ (0x5EC0DE01 + 2r)). */
+uint32_t ro_relabel(uint64_t seed, int32_t scale, uint32_t x);
+
 typedef struct {
   int32_t n;
   int64_t m;
@@ -124,10 +131,10 @@ typedef struct {
   int32_t *cols; /* m */
 } ro_csr;
 
-/* R-MAT scale/edge-factor graph, self-loops and duplicates removed,
- * symmetrised.  mode 0: oriented low-degree -> high-degree (ties by id),
- * the triangle-counting input.  mode 1: full symmetric adjacency.  Rows
- * sorted ascending. */
+/* R-MAT scale/edge-factor graph, vertices relabeled by ro_relabel (unless
+ * mode & 2), self-loops and duplicates removed, symmetrised.  mode & 1 == 0:
+ * oriented low-degree -> high-degree (ties by id), the triangle-counting
+ * input; mode & 1 == 1: full symmetric adjacency.  Rows sorted ascending. */
 ro_csr *ro_rmat_graph(int32_t scale, int32_t edge_factor, uint64_t seed,
                       double a, double b, double c, int32_t mode);
 void ro_csr_free(ro_csr *g);

@@ -131,18 +131,23 @@ class Table:
             pass
 
 
+TC_DEFAULT, TC_EDGE, TC_STAGED = 0, 1, 2
+
+
 def tc_count_async(t: Table, off: torch.Tensor, cols: torch.Tensor,
-                   out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+                   out: Optional[torch.Tensor] = None, method: int = TC_DEFAULT,
+                   stream=None) -> torch.Tensor:
     """Triangle count into a device u64 (as int64 tensor), asynchronously."""
     if out is None:
         out = torch.empty(1, dtype=torch.int64, device=cols.device)
-    check(_lib().reset_tc_count(t.handle, _ptr(off), _ptr(cols), cols.numel(),
-                                _ptr(out), _stream(stream)))
+    check(_lib().reset_tc_count_ex(t.handle, _ptr(off), _ptr(cols), cols.numel(),
+                                   method, _ptr(out), _stream(stream)))
     return out
 
 
-def tc_count(t: Table, off: torch.Tensor, cols: torch.Tensor, stream=None) -> int:
-    out = tc_count_async(t, off, cols, stream=stream)
+def tc_count(t: Table, off: torch.Tensor, cols: torch.Tensor, method: int = TC_DEFAULT,
+             stream=None) -> int:
+    out = tc_count_async(t, off, cols, method=method, stream=stream)
     return int(out.item()) & ((1 << 64) - 1)
 
 
@@ -207,11 +212,12 @@ def intersect_count(a: torch.Tensor, b: torch.Tensor, alpha: float = 0.2,
 
 def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 0x5EED0016,
              a: float = 0.57, b: float = 0.19, c: float = 0.19,
-             oriented: bool = True, stream=None):
+             oriented: bool = True, relabel: bool = True, stream=None):
     """Seeded R-MAT CSR generated on the device -> (off int32, cols int32)."""
     L = _lib()
     po, pc, m = C.c_void_p(), C.c_void_p(), C.c_int64()
-    check(L.reset_gen_rmat(scale, edge_factor, seed, a, b, c, int(bool(oriented)),
+    opts = (0 if oriented else 1) | (0 if relabel else 2)
+    check(L.reset_gen_rmat(scale, edge_factor, seed, a, b, c, opts,
                            C.byref(po), C.byref(pc), C.byref(m), _stream(stream)))
     try:
         n = 1 << scale

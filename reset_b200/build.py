@@ -22,6 +22,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libreset.so")
+HOST = os.path.join(PKG, "host")
+BIN = os.path.join(PKG, "bin")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -78,7 +81,26 @@ def build(force: bool = False, ptxas_verbose: bool = False, verbose: bool = Fals
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link of libreset.so failed")
+    build_host_tools(force)
     return LIB
+
+
+def build_host_tools(force: bool = False):
+    """C++ drop-in drivers (host/*.cpp) linked against libreset.so."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    hdrs = [os.path.join(INCLUDE, "reset.h"), os.path.join(INCLUDE, "reset.hpp")]
+    for src in sorted(glob.glob(os.path.join(HOST, "*.cpp"))):
+        exe = os.path.join(BIN, os.path.basename(src)[:-4])
+        if not force and not _stale(exe, [src, LIB] + hdrs):
+            continue
+        cmd = [cxx, "-O2", "-std=c++17", "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"),
+               src, "-o", exe, "-L", PKG, "-lreset", "-L", os.path.join(CUDA_HOME, "lib64"),
+               "-lcudart", "-Wl,-rpath,$ORIGIN/..", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"build of {os.path.basename(exe)} failed")
 
 
 def main():

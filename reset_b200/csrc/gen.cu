@@ -5,7 +5,11 @@
 // Edge i draws 2^scale x 2^scale quadrants level by level from 16-bit fields
 // of w_g = mix64(seed ^ mix64(8*i + g)) (four levels per 64-bit word, mix64
 // the splitmix64 finaliser), quadrant a/b/c/d by integer thresholds on
-// [0, 65536).  The graph is then cleaned the way the reference's
+// [0, 65536).  Vertex labels then go through a seeded bijection, as Graph500
+// permutes the labels of its Kronecker graphs: raw R-MAT ids keep the
+// quadrant bias in every bit (hubs at small ids), which would concentrate
+// keys in a few buckets of any table that hashes by id bits.  The graph is
+// then cleaned the way the reference's
 // preprocessing does it (preprocess/preprocessor.py:158-210): symmetrised,
 // self-loops and duplicates removed; for triangle counting each edge is kept
 // once, oriented from the lower (degree, id) end to the higher one.  Rows
@@ -24,8 +28,29 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
+// Seeded bijection of [0, 2^scale): vertex relabeling (Graph500 permutes
+// the labels of its Kronecker graphs the same way).  Three rounds of
+// multiply by an odd constant, xor-shift by ceil(scale/2), add a constant.
+struct Relabel {
+  uint32_t M[3], A[3], mask;
+  int sh;
+};
+
+Relabel make_relabel(uint64_t seed, int scale);
+
+__device__ __forceinline__ uint32_t relabel(const Relabel& r, uint32_t x) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    x = (x * r.M[i]) & r.mask;
+    x ^= x >> r.sh;
+    x = (x + r.A[i]) & r.mask;
+  }
+  return x;
+}
+
 __global__ void rmat_kernel(uint64_t seed, int scale, int64_t ne, int ta,
-                            int tb, int tc, uint64_t* __restrict__ keys) {
+                            int tb, int tc, int do_relabel, Relabel rl,
+                            uint64_t* __restrict__ keys) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ne;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t u = 0, v = 0;
@@ -36,6 +61,10 @@ __global__ void rmat_kernel(uint64_t seed, int scale, int64_t ne, int ta,
       const uint32_t bu = r >= tb, bv = (r >= ta && r < tb) || r >= tc;
       u = (u << 1) | bu;
       v = (v << 1) | bv;
+    }
+    if (do_relabel) {
+      u = relabel(rl, u);
+      v = relabel(rl, v);
     }
     if (u == v) {
       keys[2 * i] = keys[2 * i + 1] = ~0ull;
@@ -78,6 +107,24 @@ __global__ void cols_kernel(const uint64_t* __restrict__ keys, int64_t nk,
     cols[i] = (int32_t)(keys[i] & 0xFFFFFFFFu);
 }
 
+uint64_t host_mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+Relabel make_relabel(uint64_t seed, int scale) {
+  Relabel r;
+  r.mask = scale >= 32 ? 0xFFFFFFFFu : ((1u << scale) - 1u);
+  r.sh = (scale + 1) / 2;
+  for (int i = 0; i < 3; ++i) {
+    r.M[i] = (uint32_t)host_mix64(seed ^ (0x5EC0DE00ull + 2 * i)) | 1u;
+    r.A[i] = (uint32_t)host_mix64(seed ^ (0x5EC0DE01ull + 2 * i));
+  }
+  return r;
+}
+
 int gen_grid(int64_t items) {
   int64_t g = (items + 255) / 256, cap = (int64_t)sm_count() * 16;
   return (int)(g < 1 ? 1 : (g > cap ? cap : g));
@@ -90,7 +137,7 @@ using namespace rst;
 
 extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
                                        uint64_t seed, double a, double b,
-                                       double c, int32_t oriented,
+                                       double c, int32_t options,
                                        int32_t** d_off_out,
                                        int32_t** d_cols_out, int64_t* m_out,
                                        reset_stream_t stream) {
@@ -99,6 +146,8 @@ extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
     return arg_fail("scale must be in 1..30, edge_factor >= 1");
   if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0))
     return arg_fail("R-MAT probabilities");
+  const int32_t oriented = (options & RESET_GEN_SYMMETRIC) ? 0 : 1;
+  const int do_relabel = (options & RESET_GEN_KEEP_IDS) ? 0 : 1;
   const int64_t n = (int64_t)1 << scale;
   const int64_t ne = (int64_t)edge_factor << scale;
   if (2 * ne > INT32_MAX) return arg_fail("too many edges for one pass");
@@ -138,7 +187,8 @@ extern "C" reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor,
   GEN_CUDA(cudaMalloc(&k0, sizeof(uint64_t) * nk));
   GEN_CUDA(cudaMalloc(&k1, sizeof(uint64_t) * nk));
   GEN_CUDA(cudaMalloc(&d_cnt, sizeof(int64_t) * 2));
-  note_launch(); rmat_kernel<<<gen_grid(ne), 256, 0, st>>>(seed, scale, ne, ta, tb, tc, k0);
+  note_launch(); rmat_kernel<<<gen_grid(ne), 256, 0, st>>>(seed, scale, ne, ta, tb, tc, do_relabel,
+                                                        make_relabel(seed, scale), k0);
   GEN_CUDA(cudaGetLastError());
   cub::DoubleBuffer<uint64_t> db(k0, k1);
   size_t tb_sort = 0, tb_uniq = 0, tb_flag = 0, tb_scan = 0;

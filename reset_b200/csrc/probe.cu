@@ -21,6 +21,7 @@
 #include <climits>
 
 #include "common.cuh"
+#include "probe_common.cuh"
 
 namespace rst {
 namespace {
@@ -28,53 +29,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kIrSlice = 2048;  // candidates per IR work item
-
-enum : int32_t { kErrBadId = 4 };
-
-template <bool HIER>
-__device__ __forceinline__ bool probe_key(int x, const int32_t* __restrict__ tb,
-                                          int lg, int lg_max, int64_t bn,
-                                          int b, int32_t* status) {
-  const int l = 1 << lg;
-  int h = home_bucket<HIER>(x, lg, lg_max);
-  int k = 0;
-  const int64_t cap = (int64_t)l * b;
-  for (int64_t t = 0; t < cap; ++t) {
-    const int s = __ldg(tb + h + (int64_t)k * bn);
-    if (s == x) return true;
-    if (s == -1) return false;
-    if (++k == b) {
-      k = 0;
-      h = (h + 1) & (l - 1);
-    }
-  }
-  atomicOr(status, kErrProbeLimit);
-  return false;
-}
-
-// Warp-inclusive scan; returns the exclusive prefix and sets *total.
-__device__ __forceinline__ int warp_excl_scan(int s, int* total) {
-  const int lane = threadIdx.x & 31;
-  int incl = s;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += t;
-  }
-  *total = __shfl_sync(kFull, incl, 31);
-  return incl - s;
-}
-
-// Largest lane k with P_k <= f (P nondecreasing across lanes, P_0 = 0).
-__device__ __forceinline__ int owner_lane(int P, int f) {
-  int k = 0;
-#pragma unroll
-  for (int step = 16; step >= 1; step >>= 1) {
-    int pk = __shfl_sync(kFull, P, k + step);
-    if (pk <= f) k += step;
-  }
-  return k;
-}
 
 // Row of edge e (warp-collective).  u0 is the row of the chunk's first edge;
 // row(e) = u0 + #{j : off[u0+1+j] <= e}, searched 32 rows at a time.
@@ -97,39 +51,6 @@ __device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
     if (__all_sync(kFull, row >= 0)) break;
   }
   return row;
-}
-
-// Flattened probing of 32 (probe side, table side) pairs held one per lane.
-// For every hit, on_hit(k) is called on the lane that probed, with k the
-// lane index of the owning pair.
-template <bool HIER, class OnHit>
-__device__ __forceinline__ void flat_probe(const int32_t* __restrict__ keys,
-                                           const int32_t* __restrict__ table,
-                                           int s, int a_start, int64_t toff,
-                                           int lg, int lg_max, int64_t bn,
-                                           int b, int32_t* status,
-                                           OnHit on_hit) {
-  const int lane = threadIdx.x & 31;
-  int S;
-  const int P = warp_excl_scan(s, &S);
-  for (int base = 0; base < S; base += 32) {
-    const int f = base + lane;
-    const int k = owner_lane(P, f);
-    const int kp = __shfl_sync(kFull, P, k);
-    const int ka = __shfl_sync(kFull, a_start, k);
-    const int klg = __shfl_sync(kFull, lg, k);
-    const int64_t kt = __shfl_sync(kFull, toff, k);
-    if (f < S) {
-      const int x = __ldg(keys + ka + (f - kp));
-      if (probe_key<HIER>(x, table + kt, klg, lg_max, bn, b, status)) on_hit(k);
-    }
-  }
-}
-
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) v += __shfl_down_sync(kFull, v, o);
-  return v;
 }
 
 // ----------------------------------------------------------------- TC ----
@@ -170,8 +91,8 @@ __global__ void __launch_bounds__(kThreads)
     const int4 A = sw ? dv : du;
     const int4 B = sw ? du : dv;
     const int s = ok ? A.y : 0;
-    flat_probe<HIER>(cols, table, s, A.x, desc_toff(B), desc_lg(B), lg_max, bn,
-                     b, status, [&](int) { ++hits; });
+    hits += flat_probe<HIER>(cols, table, s, A.x, desc_toff(B), desc_lg(B),
+                             lg_max, bn, b, status, [](int) {});
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(count, hits);
@@ -419,17 +340,20 @@ using namespace rst;
 
 extern "C" {
 
-reset_status reset_tc_count(const reset_table* t, const int32_t* d_off,
-                            const int32_t* d_cols, int64_t m,
-                            uint64_t* d_count, reset_stream_t stream) {
+reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
+                               const int32_t* d_cols, int64_t m, int32_t method,
+                               uint64_t* d_count, reset_stream_t stream) {
   if (!t || !d_count) return arg_fail("NULL table or count");
   if (m < 0 || m > INT32_MAX) return arg_fail("m out of range");
   if (m > 0 && (!d_cols || !d_off)) return arg_fail("NULL offsets or cols");
+  if (method < 0 || method > 2) return arg_fail("method must be 0, 1 or 2");
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
   DescScope ds;
   RST_CHECK(resolve_desc(t, d_off, st, &ds));
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(d_count);
+  if (method != 1) return tc_staged(t, ds.desc, d_cols, m, cnt, st);
   const int32_t* rows = t->d_chunk_row;
   int32_t* owned_rows = nullptr;
   if (d_off != t->build_off || m != t->m) {
@@ -439,20 +363,26 @@ reset_status reset_tc_count(const reset_table* t, const int32_t* d_off,
   const void* k = t->hier ? (const void*)tc_kernel<true> : (const void*)tc_kernel<false>;
   const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps, persistent_grid(k));
   if (t->hier) {
-    note_launch(); tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
+    note_launch();
+    tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
         ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
-        t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
-        t->d_status);
+        t->bucket, t->lg_max, cnt, t->d_status);
   } else {
-    note_launch(); tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
+    note_launch();
+    tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
         ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
-        t->bucket, t->lg_max, reinterpret_cast<unsigned long long*>(d_count),
-        t->d_status);
+        t->bucket, t->lg_max, cnt, t->d_status);
   }
   cudaError_t e = cudaGetLastError();
   if (owned_rows) cudaFreeAsync(owned_rows, st);
   if (e != cudaSuccess) return cuda_fail(e, "tc_kernel launch", __FILE__, __LINE__);
   return RESET_OK;
+}
+
+reset_status reset_tc_count(const reset_table* t, const int32_t* d_off,
+                            const int32_t* d_cols, int64_t m,
+                            uint64_t* d_count, reset_stream_t stream) {
+  return reset_tc_count_ex(t, d_off, d_cols, m, 0, d_count, stream);
 }
 
 static reset_status sss_common(const reset_table* t, const int32_t* d_off,

@@ -64,7 +64,8 @@ def outputs(d, names):
 
 
 def tc_case(work, name, scale, seed, alpha, bucket):
-    off, cols = O.rmat_graph(scale, 16, seed, oriented=True)
+    # raw R-MAT ids (skewed bucket occupancy: long probe chains are exercised)
+    off, cols = O.rmat_graph(scale, 16, seed, oriented=True, relabel=False)
     d = os.path.join(work, name)
     os.makedirs(d, exist_ok=True)
     write_arr(f"{d}/csr_offsets_tri.bin", off)
@@ -79,7 +80,7 @@ def tc_case(work, name, scale, seed, alpha, bucket):
 
 
 def sss_case(work, name, scale, seed, thr):
-    off, cols = O.rmat_graph(scale, 16, seed, oriented=False)
+    off, cols = O.rmat_graph(scale, 16, seed, oriented=False, relabel=False)
     n = off.size - 1
     vert = np.repeat(np.arange(n, dtype=np.int32), np.diff(off))
     d = os.path.join(work, name)

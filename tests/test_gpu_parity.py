@@ -26,11 +26,13 @@ def host(t):
 
 # ------------------------------------------------------------- generator --
 
-@pytest.mark.parametrize("scale,oriented", [(6, True), (10, True), (12, False), (16, True)])
-def test_gen_rmat_matches_oracle(R, cuda, oracle_mod, scale, oriented):
+@pytest.mark.parametrize("scale,oriented,relabel", [
+    (6, True, True), (10, True, True), (12, False, True), (16, True, True),
+    (10, True, False), (12, False, False), (1, True, True), (2, False, True)])
+def test_gen_rmat_matches_oracle(R, cuda, oracle_mod, scale, oriented, relabel):
     seed = 0x5EED0000 + scale
-    off, cols = R.gen_rmat(scale, 16, seed, oriented=oriented)
-    o_off, o_cols = oracle_mod.rmat_graph(scale, 16, seed, oriented=oriented)
+    off, cols = R.gen_rmat(scale, 16, seed, oriented=oriented, relabel=relabel)
+    o_off, o_cols = oracle_mod.rmat_graph(scale, 16, seed, oriented=oriented, relabel=relabel)
     assert np.array_equal(host(off), o_off)
     assert np.array_equal(host(cols), o_cols)
 
@@ -266,3 +268,48 @@ def test_intersect_count(R, cuda, oracle_mod, na, nb, universe):
     b = rng.integers(0, universe, size=nb).astype(np.int32)
     got = R.intersect_count(dev(a, cuda), dev(b, cuda))
     assert got == oracle_mod.pair_count(a, b)
+
+
+# ------------------------------------------------- TC methods, odd shapes --
+
+def _random_rows(rng, sizes, n, dup_every=0):
+    rows = []
+    for i, s in enumerate(sizes):
+        r = rng.choice(n, size=min(s, n), replace=False) if s else np.zeros(0, np.int64)
+        if dup_every and i % dup_every == 0 and r.size > 1:
+            r = np.concatenate([r, r[: max(1, r.size // 3)]])  # repeated entries
+        rows.append(np.sort(r).astype(np.int32))
+    off = np.zeros(len(rows) + 1, np.int32)
+    off[1:] = np.cumsum([r.size for r in rows])
+    return off, np.concatenate(rows).astype(np.int32)
+
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_tc_methods_on_ragged_rows(R, cuda, oracle_mod, hier):
+    """Row lengths at every class boundary of the staged kernel (tiny < 32,
+    warp-staged <= 256, CTA-staged <= 4096, unstaged above), rows with
+    repeated entries and equal-length pairs (the probe direction decides the
+    count there), against the oracle's restatement of TC.cu:143-183."""
+    rng = np.random.default_rng(17)
+    n = 9000
+    sizes = list(rng.integers(0, 40, size=n))
+    for i, s in zip(range(0, 60, 5), [31, 32, 33, 255, 256, 257, 300, 4095, 4096, 4097, 6000, 8000]):
+        sizes[i] = s
+    off, cols = _random_rows(rng, sizes, n, dup_every=7)
+    ot = oracle_mod.Table(off, cols, hier=hier)
+    want = oracle_mod.tc_hash(ot)
+    doff, dcols = dev(off, cuda), dev(cols, cuda)
+    t = R.Table(doff, dcols, hierarchical=hier, hash_order=True)
+    for method in (R.TC_EDGE, R.TC_STAGED):
+        assert R.tc_count(t, doff, dcols, method=method) == want
+        assert R.tc_count(t, doff, t.hash_order, method=method) == oracle_mod.tc_hash(ot, ot.hash_order())
+    t.check()
+
+
+@pytest.mark.parametrize("scale", [10, 14, 17])
+def test_tc_methods_agree_rmat(R, cuda, oracle_mod, scale):
+    off, cols = R.gen_rmat(scale, 16, 0x5EED0100 + scale, oriented=True)
+    want = oracle_mod.tc_merge(off.cpu().numpy(), cols.cpu().numpy())
+    t = R.Table(off, cols, hash_order=True)
+    for method in (R.TC_EDGE, R.TC_STAGED):
+        assert R.tc_count(t, off, t.hash_order, method=method) == want

@@ -153,7 +153,7 @@ def test_oracle_matches_reference_tc(oracle_mod, name):
     alpha, b = float(g["alpha"]), int(g["bucket"])
     max_len, bucket_num, c_norm, c_hier = (int(x) for x in g["ref_meta"])
     # the inputs are re-creatable from the seed
-    o2, c2 = O.rmat_graph(int(g["scale"]), 16, int(g["seed"]), oriented=True)
+    o2, c2 = O.rmat_graph(int(g["scale"]), 16, int(g["seed"]), oriented=True, relabel=False)
     assert np.array_equal(o2, off) and np.array_equal(c2, cols)
     want = O.tc_merge(off, cols)
     assert c_norm == want and c_hier == want
@@ -217,3 +217,22 @@ def test_oracle_matches_reference_pair(oracle_mod, name):
         a, b = b, a
     _, c_norm, c_opt = (int(x) for x in g["ref_meta"])
     assert c_norm == c_opt == oracle_mod.pair_count(a, b)
+
+
+def test_relabel_is_a_bijection(oracle_mod):
+    L = oracle_mod.lib()
+    for scale in (1, 2, 5, 12):
+        img = {L.ro_relabel(0x5EED, scale, x) for x in range(1 << scale)}
+        assert img == set(range(1 << scale))
+
+
+def test_relabel_spreads_hash_buckets(oracle_mod):
+    """Raw R-MAT ids crowd a few buckets (hubs at small ids, biased bits);
+    relabeled ids fill the tables evenly."""
+    O = oracle_mod
+    for relabel, lo, hi in [(False, 0.04, 1.0), (True, 0.0, 0.01)]:
+        off, cols = O.rmat_graph(14, 16, 0x5EED0014, oriented=False, relabel=relabel)
+        t = O.Table(off, cols, hier=True)
+        occ = (t.table.reshape(t.bucket, t.bucket_num) != -1).sum(0)
+        full = float((occ == t.bucket).mean())
+        assert lo <= full <= hi, (relabel, full)
