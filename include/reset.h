@@ -137,6 +137,26 @@ reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
                                int32_t method, uint64_t *d_count,
                                reset_stream_t stream);
 
+/* reset_tc_count for callers that cannot allocate device memory while they
+ * run -- for example a serving process that has reserved nearly all HBM for
+ * resident tables, where a cudaMalloc can fail mid-request and a cudaFree
+ * synchronises the whole device and stalls every other stream.  It has no
+ * counterpart in the reference.  Same count as reset_tc_count (vertex-staged
+ * method); it calls no cudaMalloc, cudaFree or allocating library routine.
+ * Its scratch (four work counters and up to 2^20 work units, 8 MiB) is one
+ * fixed device array inside libreset.so, present on every GPU that loads the
+ * library until the process exits.  Limits: at most 134,209,536 edges (m and
+ * the table's own edge count), and d_off must be NULL or the offsets the
+ * table was built from; otherwise RESET_ERR_ARG.  The first call on a device
+ * looks up the array's device address (once per device), so make that first
+ * call before any stream capture.  All calls share the array and the array
+ * keeps the last call's contents (the counters are cleared at every call):
+ * calls that overlap on the GPU -- on different streams, or from different
+ * threads -- race on it and must be serialised by the caller. */
+reset_status reset_tc_count_noalloc(const reset_table *t, const int32_t *d_off,
+                                    const int32_t *d_cols, int64_t m,
+                                    uint64_t *d_count, reset_stream_t stream);
+
 /* Set-similarity decisions for P explicit pairs (d_pair_a[p], d_pair_b[p])
  * of sets of the table's CSR.  I = |A ∩ B| by probing the smaller set into
  * the larger set's table; U = |A| + |B| - I.

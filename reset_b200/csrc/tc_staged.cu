@@ -22,6 +22,7 @@
 //            then their probes flattened across the warp (thread-granularity
 //            work for tiny intersections).
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "probe_common.cuh"
@@ -336,3 +337,94 @@ reset_status tc_staged(const reset_table* t, const int4* desc,
 }
 
 }  // namespace rst
+
+// ---------------------------------------------------------------------------
+// reset_tc_count_noalloc: the vertex-staged count with its scratch (four work
+// counters and the (row, segment) unit list) in a fixed device array instead
+// of per-call cudaMallocAsync, for callers that must not allocate device
+// memory while they run.  The array is loaded with the library on every GPU
+// that uses it and stays until the process exits.
+// ---------------------------------------------------------------------------
+namespace rst {
+namespace {
+
+// Unit capacity: at most m/128 + 64 units are needed for m edges, so the
+// entry point accepts up to (kNoAllocUnits - 64) * 128 edges.
+constexpr int kNoAllocUnits = 1 << 20;
+constexpr int64_t kNoAllocMaxEdges = (int64_t)(kNoAllocUnits - 64) * 128;
+// [0] and [1] hold the four int32 counters; units start at [2].  8 MiB.
+static __device__ __align__(256) int2 g_tc_noalloc_scratch[kNoAllocUnits + 2];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+int2* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device; looked up once
+// per device (the host-side symbol is not a device address).
+reset_status noalloc_scratch(int2** out) {
+  int dev = 0;
+  RST_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return arg_fail("device ordinal too large");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    RST_CUDA(cudaGetSymbolAddress(&p, g_tc_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<int2*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return RESET_OK;
+}
+
+}  // namespace
+}  // namespace rst
+
+extern "C" reset_status reset_tc_count_noalloc(const reset_table* t,
+                                               const int32_t* d_off,
+                                               const int32_t* d_cols,
+                                               int64_t m, uint64_t* d_count,
+                                               reset_stream_t stream) {
+  using namespace rst;
+  if (!t || !d_count) return arg_fail("NULL table or count");
+  if (m < 0 || m > INT32_MAX) return arg_fail("m out of range");
+  if (m > 0 && !d_cols) return arg_fail("NULL cols");
+  if (d_off && d_off != t->build_off)
+    return arg_fail("reset_tc_count_noalloc needs the offsets the table was built from");
+  if (m > kNoAllocMaxEdges || t->m > kNoAllocMaxEdges) {
+    set_error("invalid argument: reset_tc_count_noalloc takes at most %lld edges "
+              "(its fixed scratch holds %d work units)",
+              (long long)kNoAllocMaxEdges, kNoAllocUnits);
+    return RESET_ERR_ARG;
+  }
+  cudaStream_t st = as_stream(stream);
+  int2* scratch = nullptr;
+  RST_CHECK(noalloc_scratch(&scratch));
+  int32_t* ctr = reinterpret_cast<int32_t*>(scratch);
+  int2* units = scratch + 2;
+  RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
+  if (m == 0 || t->n == 0) return RESET_OK;
+  RST_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int32_t) * 4, st));
+  const int g1 = (int)std::min<int64_t>((t->n + 255) / 256, (int64_t)sm_count() * 8);
+  note_launch();
+  tc_plan_kernel<<<g1 > 0 ? g1 : 1, 256, 0, st>>>(t->d_desc, t->n, units, ctr + 2,
+                                                  kNoAllocUnits, t->d_status);
+  RST_CUDA(cudaGetLastError());
+  const size_t smem = sizeof(int) * kCtaSmem;
+  const void* k = t->hier ? (const void*)tc_staged_kernel<true>
+                          : (const void*)tc_staged_kernel<false>;
+  RST_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  RST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kT, smem));
+  const int grid = sm_count() * (per_sm > 0 ? per_sm : 1);
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(d_count);
+  note_launch();
+  if (t->hier)
+    tc_staged_kernel<true><<<grid, kT, smem, st>>>(
+        t->d_desc, d_cols, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
+        t->bucket_num, t->bucket, t->lg_max, cnt, t->d_status);
+  else
+    tc_staged_kernel<false><<<grid, kT, smem, st>>>(
+        t->d_desc, d_cols, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
+        t->bucket_num, t->bucket, t->lg_max, cnt, t->d_status);
+  RST_CUDA(cudaGetLastError());
+  return RESET_OK;
+}
