@@ -58,8 +58,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--probe-rounds", type=int, default=0, choices=[0, 2, 4])
+    ap.add_argument("--warp-pair-min", type=int, default=0)
     ap.add_argument("--tc-method", type=int, default=0, choices=[0, 1, 2],
-                    help="0 default (vertex-staged), 1 edge-flattened, 2 vertex-staged")
+                    help="0 default (edge-flattened), 1 edge-flattened, 2 vertex-staged")
     return ap.parse_args()
 
 
@@ -174,6 +176,9 @@ def run_ours(a, rank, world, local):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     L = _lib.load()
+    if a.probe_rounds or a.warp_pair_min:
+        api.set_tuning(probe_rounds=a.probe_rounds or None,
+                       warp_pair_min=a.warp_pair_min or None)
 
     off, cols = api.gen_rmat(a.scale, a.edge_factor, SEED)
     n, m = off.numel() - 1, cols.numel()
@@ -284,7 +289,8 @@ def run_ours(a, rank, world, local):
                    "scale": a.scale, "edge_factor": a.edge_factor, "vertices": n,
                    "oriented_edges": m, "triangles": expect, "probes": sum_s,
                    "alpha": 0.2, "bucket": 5, "hash": "hierarchical",
-                   "tc_method": ["vertex-staged", "edge-flattened", "vertex-staged"][a.tc_method],
+                   "tc_method": ["edge-flattened", "edge-flattened", "vertex-staged"][a.tc_method],
+                   "tuning": api.get_tuning(),
                    "vertex_ids": "relabeled by a seeded bijection (Graph500 convention)",
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (tables+rows > 6 GB); no flush"},
@@ -294,7 +300,7 @@ def run_ours(a, rank, world, local):
         "probe_only": {"value": world * m / (probe_avg / 1e3), "unit": UNIT,
                        "ms_per_launch": probe_avg},
         "roofline": {"bound": "hbm",
-                     "kernel": "tc_kernel" if a.tc_method == 1 else "tc_staged_kernel",
+                     "kernel": "tc_staged_kernel" if a.tc_method == 2 else "tc_kernel",
                      "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": traffic,

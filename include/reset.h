@@ -101,8 +101,14 @@ reset_status reset_table_build(const int32_t *d_off, const int32_t *d_elems,
 reset_status reset_table_info(const reset_table *t, reset_table_view *view);
 
 /* Free a table (replaces HashTableBuilder::free_hash_tables,
- * baseline/common/hash_table.cuh:45-72).  Synchronises the device. */
+ * baseline/common/hash_table.cuh:45-72).  Synchronises the device.  Table
+ * memory comes from a library-owned stream-ordered pool that keeps freed
+ * pages mapped, so the next build of a similar table maps no new memory. */
 reset_status reset_table_free(reset_table *t);
+
+/* Returns the pages the table pool keeps for reuse to the device
+ * (no counterpart in the reference).  Synchronises the device. */
+reset_status reset_release_cached_memory(void);
 
 /* Synchronise `stream` and report device-side errors raised by kernels that
  * used this table since the last call (RESET_ERR_PROBE_LIMIT,
@@ -127,9 +133,10 @@ reset_status reset_tc_count(const reset_table *t, const int32_t *d_off,
                             uint64_t *d_count, reset_stream_t stream);
 
 /* reset_tc_count with an explicit method (same count either way):
- *   0 = default (2);
- *   1 = edge-flattened: 32 edges per warp, their probes flattened across the
- *       lanes, both sides read from HBM (the reference's access pattern);
+ *   0 = default (1, the faster on B200 as measured);
+ *   1 = edge-flattened: 32 edges per warp; pairs of >= 32 keys probed by the
+ *       whole warp, smaller ones flattened across the lanes, both sides read
+ *       from HBM (the reference's access pattern);
  *   2 = vertex-staged: each row staged once in shared memory (keys + hash
  *       set) and reused by all its out-edges. */
 reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
@@ -222,6 +229,19 @@ reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed,
                             int32_t **d_off_out, int32_t **d_cols_out,
                             int64_t *m_out, reset_stream_t stream);
 reset_status reset_free(void *d_ptr);
+
+/* ---- tuning --------------------------------------------------------------- */
+
+/* Process-wide kernel knobs (no counterpart in the reference, whose launch
+ * shapes are compile-time constants).  Results never depend on them. */
+typedef struct reset_tuning {
+  int32_t probe_rounds;  /* 2 or 4: probe rounds a warp keeps in flight     */
+  int32_t warp_pair_min; /* pairs with >= this many keys get a whole warp   */
+  int32_t reserved[6];
+} reset_tuning;
+
+reset_status reset_get_tuning(reset_tuning *out);
+reset_status reset_set_tuning(const reset_tuning *in);
 
 /* ---- misc --------------------------------------------------------------- */
 

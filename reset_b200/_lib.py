@@ -30,6 +30,11 @@ class Params(C.Structure):
                 ("reserved", C.c_int32 * 6)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("probe_rounds", C.c_int32), ("warp_pair_min", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
 class TableView(C.Structure):
     _fields_ = [("n", C.c_int32), ("bucket", C.c_int32), ("max_len", C.c_int32),
                 ("hierarchical", C.c_int32), ("bucket_num", C.c_int64),
@@ -49,6 +54,7 @@ SIGNATURES = {
                                 C.POINTER(P), P]),
     "reset_table_info": (I32, [P, C.POINTER(TableView)]),
     "reset_table_free": (I32, [P]),
+    "reset_release_cached_memory": (I32, []),
     "reset_table_check": (I32, [P, P]),
     "reset_csr_hash_order": (I32, [P, P, P, P]),
     "reset_tc_count": (I32, [P, P, P, I64, P, P]),
@@ -65,6 +71,8 @@ SIGNATURES = {
     "reset_last_error_string": (C.c_char_p, []),
     "reset_status_string": (C.c_char_p, [I32]),
     "reset_abi_version": (I32, []),
+    "reset_get_tuning": (I32, [C.POINTER(Tuning)]),
+    "reset_set_tuning": (I32, [C.POINTER(Tuning)]),
     "reset_kernel_launches": (I64, []),
 }
 

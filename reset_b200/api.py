@@ -12,7 +12,7 @@ from typing import Optional, Tuple
 
 import torch
 
-from ._lib import Params, TableView, check, load
+from ._lib import Params, TableView, Tuning, check, load
 
 
 def _lib():
@@ -228,3 +228,19 @@ def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 0x5EED0016,
         L.reset_free(po)
         L.reset_free(pc)
     return off, cols
+
+
+def get_tuning() -> dict:
+    t = Tuning()
+    check(_lib().reset_get_tuning(C.byref(t)))
+    return {"probe_rounds": t.probe_rounds, "warp_pair_min": t.warp_pair_min}
+
+
+def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] = None):
+    t = Tuning()
+    check(_lib().reset_get_tuning(C.byref(t)))
+    if probe_rounds is not None:
+        t.probe_rounds = probe_rounds
+    if warp_pair_min is not None:
+        t.warp_pair_min = warp_pair_min
+    check(_lib().reset_set_tuning(C.byref(t)))

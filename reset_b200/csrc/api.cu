@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -10,6 +11,13 @@ namespace rst {
 
 static thread_local char g_err[512] = "";
 static std::atomic<long long> g_launches{0};
+static std::mutex g_tune_mu;
+static reset_tuning g_tune = {4, 32, {0, 0, 0, 0, 0, 0}};
+
+reset_tuning tuning() {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  return g_tune;
+}
 
 void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
@@ -76,6 +84,23 @@ void reset_params_default(reset_params* p) {
   memset(p, 0, sizeof(*p));
   p->alpha = 0.2f;
   p->bucket = 5;
+}
+
+reset_status reset_get_tuning(reset_tuning* out) {
+  if (!out) return rst::arg_fail("NULL tuning");
+  *out = rst::tuning();
+  return RESET_OK;
+}
+
+reset_status reset_set_tuning(const reset_tuning* in) {
+  if (!in) return rst::arg_fail("NULL tuning");
+  if (in->probe_rounds != 2 && in->probe_rounds != 4)
+    return rst::arg_fail("probe_rounds must be 2 or 4");
+  if (in->warp_pair_min < 1 || in->warp_pair_min > (1 << 20))
+    return rst::arg_fail("warp_pair_min must be in 1..2^20");
+  std::lock_guard<std::mutex> lock(rst::g_tune_mu);
+  rst::g_tune = *in;
+  return RESET_OK;
 }
 
 reset_status reset_free(void* d_ptr) {

@@ -128,6 +128,10 @@ reset_status make_desc(const reset_table* t, const int32_t* d_off,
 reset_status make_chunk_rows(const int32_t* d_off, int32_t n, int64_t m,
                              int32_t** d_rows_out, cudaStream_t stream);
 int sm_count();
+// Process-wide kernel tuning knobs (reset_set_tuning).
+reset_tuning tuning();
+// The library-owned table memory pool of the current device.
+reset_status table_pool(cudaMemPool_t* out);
 // Vertex-staged triangle counting (tc_staged.cu); *count must be zeroed.
 reset_status tc_staged(const reset_table* t, const int4* desc,
                        const int32_t* d_cols, int64_t m,

@@ -55,22 +55,27 @@ __device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
 
 // ----------------------------------------------------------------- TC ----
 
-template <bool HIER>
+template <bool HIER, int ROUNDS>
 __global__ void __launch_bounds__(kThreads)
     tc_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ off,
               const int32_t* __restrict__ cols,
               const int32_t* __restrict__ chunk_row, int32_t n, int64_t m,
               const int32_t* __restrict__ table, int64_t bn, int b, int lg_max,
               unsigned long long* __restrict__ count,
+              unsigned long long* __restrict__ cursor, int warp_pair_min,
               int32_t* __restrict__ status) {
-  const int lane = threadIdx.x & 31;
+  __shared__ int s_qx[kWarps][32 * ROUNDS], s_qh[kWarps][32 * ROUNDS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // edges past off[n] have no row: never read them (nor their chunk rows)
   const int64_t me = min(m, (int64_t)__ldg(off + n));
   const int64_t n_chunks = (me + 31) >> 5;
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long hits = 0;
-  for (int64_t c = gw; c < n_chunks; c += nw) {
+  // dynamic schedule: a warp takes the next 32-edge chunk when it is done
+  for (;;) {
+    unsigned long long cc = 0;
+    if (lane == 0) cc = atomicAdd(cursor, 1ull);
+    const int64_t c = (int64_t)__shfl_sync(kFull, cc, 0);
+    if (c >= n_chunks) break;
     const int64_t e64 = c * 32 + lane;
     const bool valid = e64 < me;
     const int e = (int)(valid ? e64 : me - 1);
@@ -91,8 +96,24 @@ __global__ void __launch_bounds__(kThreads)
     const int4 A = sw ? dv : du;
     const int4 B = sw ? du : dv;
     const int s = ok ? A.y : 0;
-    hits += flat_probe<HIER>(cols, table, s, A.x, desc_toff(B), desc_lg(B),
-                             lg_max, bn, b, status, [](int) {});
+    // pairs with a warp's worth of keys get the whole warp, one at a time;
+    // the rest are flattened across the lanes
+    const bool big = s >= warp_pair_min;
+    unsigned bigm = __ballot_sync(kFull, big);
+    const int64_t bt = desc_toff(B);
+    const int blg = desc_lg(B);
+    while (bigm) {
+      const int k = __ffs(bigm) - 1;
+      bigm &= bigm - 1;
+      const int ks = __shfl_sync(kFull, s, k);
+      const int ka = __shfl_sync(kFull, A.x, k);
+      const int klg = __shfl_sync(kFull, blg, k);
+      const int64_t kt = __shfl_sync(kFull, bt, k);
+      hits += warp_probe_pair<HIER, ROUNDS>(cols + ka, ks, table + kt, klg, lg_max,
+                                            bn, b, status, s_qx[warp], s_qh[warp]);
+    }
+    hits += flat_probe<HIER>(cols, me, table, big ? 0 : s, A.x, bt, blg, lg_max,
+                             bn, b, status, [](int) {});
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(count, hits);
@@ -103,7 +124,7 @@ __global__ void __launch_bounds__(kThreads)
 template <bool HIER, bool FLOAT_RULE>
 __global__ void __launch_bounds__(kThreads)
     sss_kernel(const int4* __restrict__ desc, int32_t n,
-               const int32_t* __restrict__ elems,
+               const int32_t* __restrict__ elems, int64_t n_elems,
                const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
                int64_t np, const int32_t* __restrict__ table, int64_t bn, int b,
                int lg_max, int num, int den, float thr,
@@ -132,7 +153,7 @@ __global__ void __launch_bounds__(kThreads)
     const int4 B = sw ? da : dq;
     s_hits[warp][lane] = 0;
     __syncwarp();
-    flat_probe<HIER>(elems, table, ok ? A.y : 0, A.x, desc_toff(B),
+    flat_probe<HIER>(elems, n_elems, table, ok ? A.y : 0, A.x, desc_toff(B),
                      desc_lg(B), lg_max, bn, b, status,
                      [&](int k) { atomicAdd(&s_hits[warp][k], 1); });
     __syncwarp();
@@ -353,27 +374,37 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   DescScope ds;
   RST_CHECK(resolve_desc(t, d_off, st, &ds));
   unsigned long long* cnt = reinterpret_cast<unsigned long long*>(d_count);
-  if (method != 1) return tc_staged(t, ds.desc, d_cols, m, cnt, st);
+  if (method == 2) return tc_staged(t, ds.desc, d_cols, m, cnt, st);
   const int32_t* rows = t->d_chunk_row;
   int32_t* owned_rows = nullptr;
   if (d_off != t->build_off || m != t->m) {
     RST_CHECK(make_chunk_rows(d_off, t->n, m, &owned_rows, st));
     rows = owned_rows;
   }
-  const void* k = t->hier ? (const void*)tc_kernel<true> : (const void*)tc_kernel<false>;
-  const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps, persistent_grid(k));
-  if (t->hier) {
-    note_launch();
-    tc_kernel<true><<<(int)g, kThreads, 0, st>>>(
-        ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
-        t->bucket, t->lg_max, cnt, t->d_status);
-  } else {
-    note_launch();
-    tc_kernel<false><<<(int)g, kThreads, 0, st>>>(
-        ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,
-        t->bucket, t->lg_max, cnt, t->d_status);
+  unsigned long long* cursor = nullptr;
+  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&cursor), sizeof(*cursor), st));
+  cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(*cursor), st);
+  const reset_tuning tun = tuning();
+  const int wpm = tun.warp_pair_min;
+#define TC_LAUNCH(H, R)                                                        \
+  do {                                                                         \
+    const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps,        \
+                                 persistent_grid((const void*)tc_kernel<H, R>)); \
+    note_launch();                                                             \
+    tc_kernel<H, R><<<(int)g, kThreads, 0, st>>>(                              \
+        ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,      \
+        t->bucket, t->lg_max, cnt, cursor, wpm, t->d_status);                  \
+  } while (0)
+  if (e == cudaSuccess) {
+    if (t->hier) {
+      if (tun.probe_rounds == 2) TC_LAUNCH(true, 2); else TC_LAUNCH(true, 4);
+    } else {
+      if (tun.probe_rounds == 2) TC_LAUNCH(false, 2); else TC_LAUNCH(false, 4);
+    }
+    e = cudaGetLastError();
   }
-  cudaError_t e = cudaGetLastError();
+#undef TC_LAUNCH
+  cudaFreeAsync(cursor, st);
   if (owned_rows) cudaFreeAsync(owned_rows, st);
   if (e != cudaSuccess) return cuda_fail(e, "tc_kernel launch", __FILE__, __LINE__);
   return RESET_OK;
@@ -404,7 +435,7 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
                                  persistent_grid((const void*)sss_kernel<H, F>)); \
     note_launch(); sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(                           \
-        ds.desc, t->n, d_elems, d_pa, d_pb, np, t->d_table, t->bucket_num,   \
+        ds.desc, t->n, d_elems, t->m, d_pa, d_pb, np, t->d_table, t->bucket_num, \
         t->bucket, t->lg_max, num, den, thr, d_flags, d_inter, t->d_status); \
   } while (0)
   if (t->hier) {

@@ -28,6 +28,7 @@
 #include <cub/cub.cuh>
 
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -527,6 +528,43 @@ reset_status make_desc(const reset_table* t, const int32_t* d_off,
   return RESET_OK;
 }
 
+// Table memory comes from a library-owned stream-ordered pool per device
+// whose release threshold is unlimited: freeing a table keeps its pages
+// mapped for the next build, so rebuilding a multi-GB table costs no
+// cudaMalloc/cudaFree page mapping (reset_release_cached_memory() returns
+// them).
+namespace {
+constexpr int kPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kPoolDevices] = {};
+}  // namespace
+
+reset_status table_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  RST_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kPoolDevices) return arg_fail("device ordinal too large");
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    RST_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX;
+    RST_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return RESET_OK;
+}
+
+void release_pools() {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  for (int d = 0; d < kPoolDevices; ++d)
+    if (g_pool[d]) cudaMemPoolTrimTo(g_pool[d], 0);
+}
+
 }  // namespace rst
 
 using namespace rst;
@@ -535,12 +573,11 @@ namespace {
 
 void destroy(reset_table* t) {
   if (!t) return;
-  cudaFree(t->d_table);
-  cudaFree(t->d_len);
-  cudaFree(t->d_off64);
-  cudaFree(t->d_desc);
-  cudaFree(t->d_chunk_row);
-  cudaFree(t->d_status);
+  // stream-ordered frees into the table pool (callers synchronise first)
+  void* ptrs[] = {t->d_table, t->d_len, t->d_off64, t->d_desc, t->d_chunk_row,
+                  t->d_status};
+  for (void* p : ptrs)
+    if (p) cudaFreeAsync(p, 0);
   delete t;
 }
 
@@ -612,11 +649,12 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   reset_status rs = RESET_OK;
   auto fail = [&](reset_status s) {
     cudaStreamSynchronize(st);
-    cudaFree(d_info);
-    cudaFree(d_big);
-    cudaFree(d_tile_first);
-    cudaFree(d_bn);
-    cudaFree(d_tmp);
+    if (d_info) cudaFreeAsync(d_info, st);
+    if (d_big) cudaFreeAsync(d_big, st);
+    if (d_tile_first) cudaFreeAsync(d_tile_first, st);
+    if (d_bn) cudaFreeAsync(d_bn, st);
+    if (d_tmp) cudaFreeAsync(d_tmp, st);
+    cudaStreamSynchronize(st);
     destroy(t);
     return s;
   };
@@ -626,14 +664,21 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
     if (_e != cudaSuccess) return fail(cuda_fail(_e, #call, __FILE__, __LINE__)); \
   } while (0)
 
-  BUILD_CUDA(cudaMalloc(&t->d_status, sizeof(int32_t)));
+  cudaMemPool_t pool;
+  {
+    reset_status ps = table_pool(&pool);
+    if (ps != RESET_OK) return fail(ps);
+  }
+#define POOL_ALLOC(ptr, bytes) \
+  BUILD_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&(ptr)), (bytes), pool, st))
+  POOL_ALLOC(t->d_status, sizeof(int32_t));
   BUILD_CUDA(cudaMemsetAsync(t->d_status, 0, sizeof(int32_t), st));
-  BUILD_CUDA(cudaMalloc(&t->d_len, sizeof(int32_t) * (n > 0 ? n : 1)));
-  BUILD_CUDA(cudaMalloc(&t->d_off64, sizeof(int64_t) * (n + 1)));
-  BUILD_CUDA(cudaMalloc(&d_info, sizeof(int32_t) * 4));
-  BUILD_CUDA(cudaMalloc(&d_bn, sizeof(int64_t)));
+  POOL_ALLOC(t->d_len, sizeof(int32_t) * (n > 0 ? n : 1));
+  POOL_ALLOC(t->d_off64, sizeof(int64_t) * (n + 1));
+  POOL_ALLOC(d_info, sizeof(int32_t) * 4);
+  POOL_ALLOC(d_bn, sizeof(int64_t));
   BUILD_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int32_t) * 4, st));
-  BUILD_CUDA(cudaMalloc(&d_big, sizeof(int32_t) * (n > 0 ? n : 1)));
+  POOL_ALLOC(d_big, sizeof(int32_t) * (n > 0 ? n : 1));
 
   if (n > 0) {
     note_launch(); meta_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_off, n, p.alpha, p.bucket,
@@ -643,7 +688,7 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
     size_t tmp_bytes = 0;
     BUILD_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, t->d_off64,
                                              t->d_off64, n, st));
-    BUILD_CUDA(cudaMalloc(&d_tmp, tmp_bytes));
+    POOL_ALLOC(d_tmp, tmp_bytes);
     BUILD_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, t->d_off64,
                                              t->d_off64, n, st));
   }
@@ -661,15 +706,14 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   if (bn >= ((int64_t)1 << 56)) return fail(arg_fail("table too large"));
 
   size_t tbytes = sizeof(int32_t) * (size_t)bn * p.bucket;
-  BUILD_CUDA(cudaMalloc(&t->d_table, tbytes > 0 ? tbytes : 16));
-  BUILD_CUDA(cudaMalloc(&t->d_desc, sizeof(int4) * (n > 0 ? n : 1)));
+  POOL_ALLOC(t->d_table, tbytes > 0 ? tbytes : 16);
+  POOL_ALLOC(t->d_desc, sizeof(int4) * (n > 0 ? n : 1));
   t->n_chunks = (m + 31) / 32;
-  BUILD_CUDA(cudaMalloc(&t->d_chunk_row,
-                        sizeof(int32_t) * (t->n_chunks > 0 ? t->n_chunks : 1)));
+  POOL_ALLOC(t->d_chunk_row, sizeof(int32_t) * (t->n_chunks > 0 ? t->n_chunks : 1));
   const int64_t n_tiles64 = (bn + g.T - 1) / g.T;
   if (n_tiles64 > INT32_MAX) return fail(arg_fail("too many tiles"));
   const int32_t n_tiles = (int32_t)n_tiles64;
-  BUILD_CUDA(cudaMalloc(&d_tile_first, sizeof(int32_t) * (n_tiles + 1)));
+  POOL_ALLOC(d_tile_first, sizeof(int32_t) * (n_tiles + 1));
   if (n > 0) {
     note_launch(); layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
         d_off, t->d_off64, t->d_len, n, t->d_desc, t->d_chunk_row,
@@ -688,6 +732,7 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   cudaFreeAsync(d_tile_first, st);
   cudaFreeAsync(d_bn, st);
   if (d_tmp) cudaFreeAsync(d_tmp, st);
+#undef POOL_ALLOC
 #undef BUILD_CUDA
   *out = t;
   return RESET_OK;
@@ -714,6 +759,12 @@ reset_status reset_table_free(reset_table* t) {
   cudaError_t e = cudaDeviceSynchronize();
   destroy(t);
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize", __FILE__, __LINE__);
+  return RESET_OK;
+}
+
+reset_status reset_release_cached_memory(void) {
+  RST_CUDA(cudaDeviceSynchronize());
+  release_pools();
   return RESET_OK;
 }
 

@@ -38,6 +38,7 @@ constexpr int kCtaMax = 4096;
 constexpr int kSeg = 256;
 constexpr int kWarpSmem = 3 * kWarpMax;       // K + H per warp (ints)
 constexpr int kCtaSmem = 3 * kCtaMax;         // K + H per CTA (ints)
+constexpr int kRounds = 4;                    // probe rounds issued together
 static_assert(kW * kWarpSmem <= kCtaSmem, "warp regions must fit the CTA buffer");
 
 __device__ __forceinline__ int hslot(int x, int lgP) {
@@ -101,21 +102,42 @@ __device__ __forceinline__ int staged_batch(
   const int lg = desc_lg(dv);
   int S;
   const int P = warp_excl_scan(s, &S);
-  for (int base = 0; base < S; base += 32) {
-    const int f = base + lane;
-    const int k = owner_lane(P, f);
-    const int kp = __shfl_sync(kFull, P, k);
-    const int ks = __shfl_sync(kFull, src, k);
-    const bool kst = __shfl_sync(kFull, (int)stream, k);
-    const int klg = __shfl_sync(kFull, lg, k);
-    const int64_t kt = __shfl_sync(kFull, toff, k);
-    if (f < S) {
+  // kRounds rounds at once: key loads (HBM for streamed rows, shared memory
+  // for u's own keys), then the first-slot loads of the table probes, then
+  // the lookups and continuations.
+  for (int base = 0; base < S; base += 32 * kRounds) {
+    int x[kRounds], h[kRounds], klg[kRounds], s0[kRounds], s1[kRounds];
+    const int32_t* tb[kRounds];
+    bool act[kRounds], kst[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      const int f = base + r * 32 + lane;
+      const int k = owner_lane(P, f);
+      const int kp = __shfl_sync(kFull, P, k);
+      const int ks = __shfl_sync(kFull, src, k);
+      kst[r] = __shfl_sync(kFull, (int)stream, k);
+      klg[r] = __shfl_sync(kFull, lg, k);
+      tb[r] = table + __shfl_sync(kFull, toff, k);
+      act[r] = f < S;
       const int jj = f - kp;
+      x[r] = act[r] ? (kst[r] ? __ldg(cols + ks + jj) : K[jj]) : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      h[r] = home_bucket<HIER>(x[r], klg[r], lg_max);
+      const bool g = act[r] && !kst[r];
+      s0[r] = g ? __ldg(tb[r] + h[r]) : -1;
+      s1[r] = g ? __ldg(tb[r] + h[r] + (b > 1 ? bn : 0)) : -1;
+    }
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      if (!act[r]) continue;
       bool hit;
-      if (kst) {
-        hit = hset_has(H, lgP, __ldg(cols + ks + jj));
+      if (kst[r]) {
+        hit = hset_has(H, lgP, x[r]);
       } else {
-        hit = probe_key<HIER>(K[jj], table + kt, klg, lg_max, bn, b, status);
+        hit = probe_resolve2<HIER>(x[r], s0[r], s1[r], tb[r], klg[r], h[r], bn, b,
+                                   status);
       }
       hits += hit;
     }
@@ -127,7 +149,7 @@ __device__ __forceinline__ int staged_batch(
 // in HBM, as in the reference kernel.
 template <bool HIER>
 __device__ __forceinline__ int global_batch(
-    int j0, int je, int4 du4, const int32_t* __restrict__ cols,
+    int j0, int je, int4 du4, const int32_t* __restrict__ cols, int64_t n_cols,
     const int4* __restrict__ desc, int n, const int32_t* __restrict__ table,
     int64_t bn, int b, int lg_max, int32_t* status) {
   const int lane = threadIdx.x & 31;
@@ -144,14 +166,14 @@ __device__ __forceinline__ int global_batch(
   const bool sw = du4.y > dv.y;
   const int4 A = sw ? dv : du4;
   const int4 B = sw ? du4 : dv;
-  return flat_probe<HIER>(cols, table, ok ? A.y : 0, A.x, desc_toff(B),
+  return flat_probe<HIER>(cols, n_cols, table, ok ? A.y : 0, A.x, desc_toff(B),
                           desc_lg(B), lg_max, bn, b, status, [](int) {});
 }
 
 template <bool HIER>
 __global__ void __launch_bounds__(kT, 2)
     tc_staged_kernel(const int4* __restrict__ desc,
-                     const int32_t* __restrict__ cols, int32_t n,
+                     const int32_t* __restrict__ cols, int64_t n_cols, int32_t n,
                      const int2* __restrict__ units,
                      const int32_t* __restrict__ n_units_p, int units_cap,
                      int32_t* __restrict__ cursors,
@@ -190,8 +212,8 @@ __global__ void __launch_bounds__(kT, 2)
                                    bn, b, lg_max, status);
     } else {
       for (int j0 = e0 + warp * 32; j0 < e1; j0 += kT)
-        hits += global_batch<HIER>(j0, e1, du4, cols, desc, n, table, bn, b,
-                                   lg_max, status);
+        hits += global_batch<HIER>(j0, e1, du4, cols, n_cols, desc, n, table, bn,
+                                   b, lg_max, status);
     }
     __syncthreads();
   }
@@ -239,8 +261,8 @@ __global__ void __launch_bounds__(kT, 2)
         const int a_start = sw ? dv.x : ksu;
         const int64_t t_off = sw ? kut : desc_toff(dv);
         const int t_lg = sw ? kulg : desc_lg(dv);
-        hits += flat_probe<HIER>(cols, table, s, a_start, t_off, t_lg, lg_max,
-                                 bn, b, status, [](int) {});
+        hits += flat_probe<HIER>(cols, n_cols, table, s, a_start, t_off, t_lg,
+                                 lg_max, bn, b, status, [](int) {});
       }
     }
     // medium rows: stage one row at a time in this warp's region
@@ -321,11 +343,11 @@ reset_status tc_staged(const reset_table* t, const int4* desc,
       note_launch();
       if (t->hier)
         tc_staged_kernel<true><<<grid, kT, smem, st>>>(
-            desc, d_cols, t->n, units, ctr + 2, cap, ctr, t->d_table,
+            desc, d_cols, m, t->n, units, ctr + 2, cap, ctr, t->d_table,
             t->bucket_num, t->bucket, t->lg_max, count, t->d_status);
       else
         tc_staged_kernel<false><<<grid, kT, smem, st>>>(
-            desc, d_cols, t->n, units, ctr + 2, cap, ctr, t->d_table,
+            desc, d_cols, m, t->n, units, ctr + 2, cap, ctr, t->d_table,
             t->bucket_num, t->bucket, t->lg_max, count, t->d_status);
       e = cudaGetLastError();
     }
@@ -419,11 +441,11 @@ extern "C" reset_status reset_tc_count_noalloc(const reset_table* t,
   note_launch();
   if (t->hier)
     tc_staged_kernel<true><<<grid, kT, smem, st>>>(
-        t->d_desc, d_cols, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
+        t->d_desc, d_cols, m, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
         t->bucket_num, t->bucket, t->lg_max, cnt, t->d_status);
   else
     tc_staged_kernel<false><<<grid, kT, smem, st>>>(
-        t->d_desc, d_cols, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
+        t->d_desc, d_cols, m, t->n, units, ctr + 2, kNoAllocUnits, ctr, t->d_table,
         t->bucket_num, t->bucket, t->lg_max, cnt, t->d_status);
   RST_CUDA(cudaGetLastError());
   return RESET_OK;
