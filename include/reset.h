@@ -186,6 +186,43 @@ reset_status reset_sss_float(const reset_table *t, const int32_t *d_off,
                              float thr, uint8_t *d_flags, int32_t *d_inter,
                              reset_stream_t stream);
 
+/* Batched set-similarity form.  A reset_batch owns device pair buffers for
+ * up to `capacity` pairs over one table and a captured CUDA graph of the
+ * persistent pair kernel; reset_batch_run decides the first `npairs` pairs
+ * of those buffers with one graph replay (no allocation, no per-batch
+ * launch setup).  Decisions are those of reset_sss with the num/den given
+ * at creation.  The caller fills *d_pair_a / *d_pair_b (from
+ * reset_batch_buffers) on `stream` or before the call; results land in
+ * *d_flags / *d_inter.  A batch belongs to one thread at a time.
+ * The batched counterpart of the reference's per-call SSS launch
+ * (set-similarity-search/sss.cu:93-154 with the host loop of
+ * set-similarity-search/main.cu). */
+typedef struct reset_batch reset_batch;
+reset_status reset_batch_create(const reset_table *t, const int32_t *d_elems,
+                                int64_t capacity, int32_t num, int32_t den,
+                                reset_batch **out, reset_stream_t stream);
+reset_status reset_batch_buffers(reset_batch *b, int32_t **d_pair_a,
+                                 int32_t **d_pair_b, uint8_t **d_flags,
+                                 int32_t **d_inter);
+reset_status reset_batch_run(reset_batch *b, int64_t npairs,
+                             reset_stream_t stream);
+reset_status reset_batch_destroy(reset_batch *b);
+
+/* Prefix-filter candidates for a Jaccard self-join at threshold num/den
+ * over token sets (d_off[n+1], d_tokens; tokens in [0, 2^universe_log2),
+ * distinct within a set).  Tokens are ordered globally by (frequency, id);
+ * set x's prefix is its first |x| - ceil(num*|x|/den) + 1 tokens in that
+ * order.  A pair (a < b) is a candidate iff the prefixes share a token and
+ * den*min(|a|,|b|) >= num*max(|a|,|b|); every pair with Jaccard >= num/den
+ * is a candidate.  Outputs: distinct pairs sorted by (a, b), allocated with
+ * cudaMalloc, owned by the caller.  n < 2^21, set sizes < 2^15.
+ * Synchronises `stream`. */
+reset_status reset_prefix_candidates(const int32_t *d_off, const int32_t *d_tokens,
+                                     int32_t n, int64_t m, int32_t universe_log2,
+                                     int32_t num, int32_t den, int32_t **d_pa_out,
+                                     int32_t **d_pb_out, int64_t *np_out,
+                                     reset_stream_t stream);
+
 /* Conjunctive retrieval.  The table is built over the inverted index
  * (d_toff[nterms+1], d_docs).  Query q is the term list
  * d_query[d_qoff[q] .. d_qoff[q+1]); its result is the posting list of its
@@ -228,6 +265,17 @@ reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed,
                             double a, double b, double c, int32_t options,
                             int32_t **d_off_out, int32_t **d_cols_out,
                             int64_t *m_out, reset_stream_t stream);
+
+/* Seeded token sets (stand-in for the set-similarity datasets): n sets,
+ * set sizes Zipf(size_s) on [size_lo, size_hi], tokens drawn from a
+ * Zipf(1)-like law over 2^universe_log2 ranks and relabeled by a seeded
+ * bijection; duplicates removed, rows sorted.  Outputs allocated with
+ * cudaMalloc, owned by the caller.  n < 2^21, size_hi <= 16384,
+ * universe_log2 in 4..24.  Synchronises `stream`. */
+reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2, double size_s,
+                                  int32_t size_lo, int32_t size_hi, uint64_t seed,
+                                  int32_t **d_off_out, int32_t **d_tokens_out,
+                                  int64_t *m_out, reset_stream_t stream);
 reset_status reset_free(void *d_ptr);
 
 /* ---- tuning --------------------------------------------------------------- */

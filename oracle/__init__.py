@@ -81,6 +81,9 @@ def lib():
         L.ro_ir.restype = None
         L.ro_pair_count.argtypes = [_i32p, C.c_int64, _i32p, C.c_int64]
         L.ro_pair_count.restype = C.c_int64
+        L.ro_jaccard_join.argtypes = [C.c_int32, _i32p, _i32p, C.c_int32,
+                                      C.c_int32, _i32p, _i32p, C.c_int64]
+        L.ro_jaccard_join.restype = C.c_int64
         L.ro_relabel.argtypes = [C.c_uint64, C.c_int32, C.c_uint32]
         L.ro_relabel.restype = C.c_uint32
         L.ro_mix64.argtypes = [C.c_uint64]
@@ -207,6 +210,51 @@ def pair_count(a, b) -> int:
     b = _c(b, np.int32)
     return int(lib().ro_pair_count(a if a.size else np.zeros(1, np.int32), a.size,
                                    b if b.size else np.zeros(1, np.int32), b.size))
+
+
+def jaccard_join(off, tok, num=7, den=10):
+    """All pairs a < b with den*I >= num*U, U > 0 (brute force; small n)."""
+    off = _c(off, np.int32)
+    tok = _c(tok, np.int32)
+    n = off.size - 1
+    cap = n * (n - 1) // 2 + 1
+    pa = np.zeros(cap, np.int32)
+    pb = np.zeros(cap, np.int32)
+    k = int(lib().ro_jaccard_join(n, off, tok if tok.size else np.zeros(1, np.int32),
+                                  num, den, pa, pb, cap))
+    return pa[:k], pb[:k]
+
+
+def prefix_candidates(off, tok, num=7, den=10):
+    """Restated prefix filter: tokens ranked by (min(freq, 2^19-1), id);
+    prefix of x = first |x| - ceil(num|x|/den) + 1 tokens in that order;
+    candidates = pairs a < b sharing a prefix token with
+    den*min(|a|,|b|) >= num*max(|a|,|b|).  Returns (pa, pb) sorted."""
+    off = np.asarray(off, np.int64)
+    tok = np.asarray(tok, np.int64)
+    n = off.size - 1
+    sz = np.diff(off)
+    freq = np.bincount(tok, minlength=int(tok.max()) + 1 if tok.size else 1)
+    freq = np.minimum(freq, (1 << 19) - 1)
+    by_token = {}
+    for x in range(n):
+        row = tok[off[x]:off[x + 1]]
+        order = row[np.lexsort((row, freq[row]))]
+        p = int(sz[x] - (num * sz[x] + den - 1) // den + 1) if sz[x] > 0 else 0
+        for t in order[:p].tolist():
+            by_token.setdefault(t, []).append(x)
+    out = set()
+    for sets in by_token.values():
+        for i in range(len(sets)):
+            for j in range(i + 1, len(sets)):
+                a, b = sets[i], sets[j]
+                lo, hi = min(sz[a], sz[b]), max(sz[a], sz[b])
+                if den * lo >= num * hi:
+                    out.add((min(a, b), max(a, b)))
+    if not out:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32)
+    arr = np.array(sorted(out), np.int32)
+    return arr[:, 0].copy(), arr[:, 1].copy()
 
 
 # ------------------------------------------------------------- generators ---

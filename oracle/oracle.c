@@ -381,6 +381,39 @@ int64_t ro_pair_count(const int32_t *a, int64_t na, const int32_t *b,
   return c;
 }
 
+/* Brute-force Jaccard self-join over sorted token sets: every pair a < b
+ * with |A| + |B| - I > 0 and den * I >= num * (|A| + |B| - I), I by a merge
+ * of the two sorted rows.  Writes at most `cap` pairs; returns the number of
+ * qualifying pairs (which may exceed cap).  Test-size inputs only
+ * (quadratic).  The set-similarity rule of set-similarity-search/sss.cu:
+ * 139-141 in its integer form, applied to all pairs. */
+int64_t ro_jaccard_join(int32_t n, const int32_t *off, const int32_t *tok,
+                        int32_t num, int32_t den, int32_t *pa, int32_t *pb,
+                        int64_t cap) {
+  int64_t k = 0;
+  for (int32_t a = 0; a < n; a++) {
+    const int32_t *ra = tok + off[a];
+    const int64_t na = off[a + 1] - off[a];
+    for (int32_t b = a + 1; b < n; b++) {
+      const int32_t *rb = tok + off[b];
+      const int64_t nb = off[b + 1] - off[b];
+      if (na + nb == 0) continue;
+      int64_t i = 0, j = 0, inter = 0;
+      while (i < na && j < nb) {
+        if (ra[i] < rb[j]) i++;
+        else if (ra[i] > rb[j]) j++;
+        else { inter++; i++; j++; }
+      }
+      const int64_t uni = na + nb - inter;
+      if ((int64_t)den * inter >= (int64_t)num * uni) {
+        if (k < cap) { pa[k] = a; pb[k] = b; }
+        k++;
+      }
+    }
+  }
+  return k;
+}
+
 /* ------------------------------------------------------------------------ */
 /* synthetic inputs                                                          */
 /* ------------------------------------------------------------------------ */

@@ -106,6 +106,12 @@ void ro_ir(int32_t nterms, const int32_t *toff, const int32_t *docs,
 int64_t ro_pair_count(const int32_t *a, int64_t na, const int32_t *b,
                       int64_t nb);
 
+/* All pairs a < b of sorted token sets with den*I >= num*U (U > 0); writes
+ * at most cap pairs in (a, b) order, returns the full count. */
+int64_t ro_jaccard_join(int32_t n, const int32_t *off, const int32_t *tok,
+                        int32_t num, int32_t den, int32_t *pa, int32_t *pb,
+                        int64_t cap);
+
 /* ---- synthetic inputs --------------------------------------------------- */
 
 /* splitmix64 finaliser; the R-MAT draw for edge i uses 16-bit fields of

@@ -67,6 +67,15 @@ SIGNATURES = {
     "reset_gen_rmat": (I32, [I32, I32, C.c_uint64, C.c_double, C.c_double,
                              C.c_double, I32, C.POINTER(P), C.POINTER(P),
                              C.POINTER(I64), P]),
+    "reset_batch_create": (I32, [P, P, I64, I32, I32, C.POINTER(P), P]),
+    "reset_batch_buffers": (I32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P),
+                                  C.POINTER(P)]),
+    "reset_batch_run": (I32, [P, I64, P]),
+    "reset_batch_destroy": (I32, [P]),
+    "reset_gen_token_sets": (I32, [I32, I32, C.c_double, I32, I32, C.c_uint64,
+                                   C.POINTER(P), C.POINTER(P), C.POINTER(I64), P]),
+    "reset_prefix_candidates": (I32, [P, P, I32, I64, I32, I32, I32, C.POINTER(P),
+                                      C.POINTER(P), C.POINTER(I64), P]),
     "reset_free": (I32, [P]),
     "reset_last_error_string": (C.c_char_p, []),
     "reset_status_string": (C.c_char_p, [I32]),

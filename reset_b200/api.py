@@ -244,3 +244,94 @@ def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] 
     if warp_pair_min is not None:
         t.warp_pair_min = warp_pair_min
     check(_lib().reset_set_tuning(C.byref(t)))
+
+
+class Batch:
+    """Batched set-similarity decisions over one table (reset_batch_*): a
+    captured CUDA graph of the persistent pair kernel with device pair
+    buffers for up to `capacity` pairs.  Fill `pair_a` / `pair_b` (views of
+    the batch's own buffers), call run(npairs), read `flags` / `inter`."""
+
+    def __init__(self, t: Table, elems: torch.Tensor, capacity: int, num: int = 7,
+                 den: int = 10, stream=None):
+        _need(elems, torch.int32, "elems")
+        self._table = t          # the batch reads the table's device arrays
+        self._elems = elems
+        self.capacity = int(capacity)
+        h = C.c_void_p()
+        check(_lib().reset_batch_create(t.handle, _ptr(elems), self.capacity, num, den,
+                                        C.byref(h), _stream(stream)))
+        self._h = h
+        pa, pb, fl, it = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(_lib().reset_batch_buffers(h, C.byref(pa), C.byref(pb), C.byref(fl),
+                                         C.byref(it)))
+        self.pair_a = _view(pa.value, self.capacity, torch.int32)
+        self.pair_b = _view(pb.value, self.capacity, torch.int32)
+        self.inter = _view(it.value, self.capacity, torch.int32)
+        self.flags = torch.as_tensor(_CudaArray(fl.value, self.capacity, "|u1"),
+                                     device="cuda")
+
+    def run(self, npairs: int, stream=None):
+        check(_lib().reset_batch_run(self._h, int(npairs), _stream(stream)))
+
+    def __call__(self, pa: torch.Tensor, pb: torch.Tensor, stream=None):
+        """Copy pairs in, run, and return (flags, inter) views of length P."""
+        P = pa.numel()
+        if P > self.capacity:
+            raise ValueError(f"{P} pairs exceed the batch capacity {self.capacity}")
+        s = stream if stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self.pair_a[:P].copy_(pa, non_blocking=True)
+            self.pair_b[:P].copy_(pb, non_blocking=True)
+        self.run(P, s)
+        return self.flags[:P], self.inter[:P]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(_lib().reset_batch_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_token_sets(n: int, universe_log2: int = 20, size_s: float = 1.6,
+                   size_lo: int = 8, size_hi: int = 512, seed: int = 0x5EED0033,
+                   stream=None):
+    """Seeded token sets on the device -> (off int32[n+1], tokens int32)."""
+    L = _lib()
+    po, pt, m = C.c_void_p(), C.c_void_p(), C.c_int64()
+    check(L.reset_gen_token_sets(n, universe_log2, size_s, size_lo, size_hi, seed,
+                                 C.byref(po), C.byref(pt), C.byref(m), _stream(stream)))
+    try:
+        off = _view(po.value, n + 1, torch.int32).clone()
+        tok = _view(pt.value, m.value, torch.int32).clone()
+        torch.cuda.current_stream().synchronize()
+    finally:
+        L.reset_free(po)
+        L.reset_free(pt)
+    return off, tok
+
+
+def prefix_candidates(off: torch.Tensor, tokens: torch.Tensor, universe_log2: int,
+                      num: int = 7, den: int = 10, stream=None):
+    """Prefix-filter candidate pairs (a < b, sorted) -> (pa, pb) int32."""
+    _need(off, torch.int32, "off")
+    _need(tokens, torch.int32, "tokens")
+    L = _lib()
+    pa, pb, npr = C.c_void_p(), C.c_void_p(), C.c_int64()
+    check(L.reset_prefix_candidates(_ptr(off), _ptr(tokens), off.numel() - 1,
+                                    tokens.numel(), universe_log2, num, den,
+                                    C.byref(pa), C.byref(pb), C.byref(npr),
+                                    _stream(stream)))
+    try:
+        a = _view(pa.value, npr.value, torch.int32).clone()
+        b = _view(pb.value, npr.value, torch.int32).clone()
+        torch.cuda.current_stream().synchronize()
+    finally:
+        L.reset_free(pa)
+        L.reset_free(pb)
+    return a, b

@@ -12,7 +12,7 @@ namespace rst {
 static thread_local char g_err[512] = "";
 static std::atomic<long long> g_launches{0};
 static std::mutex g_tune_mu;
-static reset_tuning g_tune = {4, 32, {0, 0, 0, 0, 0, 0}};
+static reset_tuning g_tune = {4, 64, {0, 0, 0, 0, 0, 0}};
 
 reset_tuning tuning() {
   std::lock_guard<std::mutex> lock(g_tune_mu);

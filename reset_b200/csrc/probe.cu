@@ -126,16 +126,29 @@ __global__ void __launch_bounds__(kThreads)
     sss_kernel(const int4* __restrict__ desc, int32_t n,
                const int32_t* __restrict__ elems, int64_t n_elems,
                const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
-               int64_t np, const int32_t* __restrict__ table, int64_t bn, int b,
-               int lg_max, int num, int den, float thr,
+               int64_t np, const int64_t* __restrict__ np_dev,
+               unsigned long long* __restrict__ cursor,
+               const int32_t* __restrict__ table, int64_t bn, int b,
+               int lg_max, int num, int den, float thr, int warp_pair_min,
                uint8_t* __restrict__ flags, int32_t* __restrict__ inter,
                int32_t* __restrict__ status) {
   __shared__ int s_hits[kWarps][32];
+  __shared__ int s_qx[kWarps][32 * 4], s_qh[kWarps][32 * 4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (np_dev) np = *np_dev;  // pair count set on the device (captured graphs)
   const int64_t n_chunks = (np + 31) >> 5;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t c = gw; c < n_chunks; c += nw) {
+  for (int64_t it = 0;; ++it) {
+    int64_t c;
+    if (cursor) {  // dynamic schedule: next chunk of 32 pairs
+      unsigned long long cc = 0;
+      if (lane == 0) cc = atomicAdd(cursor, 1ull);
+      c = (int64_t)__shfl_sync(kFull, cc, 0);
+    } else {
+      c = gw + it * nw;
+    }
+    if (c >= n_chunks) break;
     const int64_t p = c * 32 + lane;
     const bool valid = p < np;
     int a = valid ? __ldg(pa + p) : 0;
@@ -151,11 +164,29 @@ __global__ void __launch_bounds__(kThreads)
     const bool sw = da.y > dq.y;  // sss.cu:108-115
     const int4 A = sw ? dq : da;
     const int4 B = sw ? da : dq;
+    const int s = ok ? A.y : 0;
     s_hits[warp][lane] = 0;
     __syncwarp();
-    flat_probe<HIER>(elems, n_elems, table, ok ? A.y : 0, A.x, desc_toff(B),
-                     desc_lg(B), lg_max, bn, b, status,
-                     [&](int k) { atomicAdd(&s_hits[warp][k], 1); });
+    // pairs with a warp's worth of keys: the whole warp, one pair at a time
+    const bool big = s >= warp_pair_min;
+    unsigned bigm = __ballot_sync(kFull, big);
+    const int64_t bt = desc_toff(B);
+    const int blg = desc_lg(B);
+    while (bigm) {
+      const int k = __ffs(bigm) - 1;
+      bigm &= bigm - 1;
+      const int ks = __shfl_sync(kFull, s, k);
+      const int ka = __shfl_sync(kFull, A.x, k);
+      const int klg = __shfl_sync(kFull, blg, k);
+      const int64_t kt = __shfl_sync(kFull, bt, k);
+      int h = warp_probe_pair<HIER, 4>(elems + ka, ks, table + kt, klg, lg_max, bn,
+                                       b, status, s_qx[warp], s_qh[warp]);
+      h = __reduce_add_sync(kFull, h);
+      if (lane == 0) s_hits[warp][k] += h;
+      __syncwarp();
+    }
+    flat_probe<HIER>(elems, n_elems, table, big ? 0 : s, A.x, bt, blg, lg_max, bn,
+                     b, status, [&](int k) { atomicAdd(&s_hits[warp][k], 1); });
     __syncwarp();
     const int I = s_hits[warp][lane];
     __syncwarp();
@@ -355,6 +386,33 @@ reset_status resolve_desc(const reset_table* t, const int32_t* d_off,
 }
 
 }  // namespace
+
+// Persistent pair kernel for the batched form: pair count read on the device
+// (np_dev), dynamic 32-pair chunks (cursor, zeroed by the caller), exact
+// rule.  No allocation and no synchronisation, so it can be captured.
+reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
+                                   const int32_t* pa, const int32_t* pb,
+                                   const int64_t* np_dev,
+                                   unsigned long long* cursor, int64_t capacity,
+                                   int32_t num, int32_t den, uint8_t* flags,
+                                   int32_t* inter, cudaStream_t st) {
+  const int wpm = tuning().warp_pair_min;
+#define SSS_P(H)                                                               \
+  do {                                                                         \
+    const int64_t g = clamp_grid(((capacity + 31) / 32 + kWarps - 1) / kWarps, \
+                                 persistent_grid((const void*)sss_kernel<H, false>)); \
+    note_launch();                                                             \
+    sss_kernel<H, false><<<(int)g, kThreads, 0, st>>>(                         \
+        t->d_desc, t->n, elems, t->m, pa, pb, capacity, np_dev, cursor,        \
+        t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, 0.f, wpm,   \
+        flags, inter, t->d_status);                                            \
+  } while (0)
+  if (t->hier) SSS_P(true); else SSS_P(false);
+#undef SSS_P
+  RST_CUDA(cudaGetLastError());
+  return RESET_OK;
+}
+
 }  // namespace rst
 
 using namespace rst;
@@ -434,9 +492,10 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   do {                                                                       \
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
                                  persistent_grid((const void*)sss_kernel<H, F>)); \
-    note_launch(); sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(                           \
-        ds.desc, t->n, d_elems, t->m, d_pa, d_pb, np, t->d_table, t->bucket_num, \
-        t->bucket, t->lg_max, num, den, thr, d_flags, d_inter, t->d_status); \
+    note_launch(); sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(             \
+        ds.desc, t->n, d_elems, t->m, d_pa, d_pb, np, nullptr, nullptr,      \
+        t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, thr,       \
+        tuning().warp_pair_min, d_flags, d_inter, t->d_status);               \
   } while (0)
   if (t->hier) {
     if (float_rule) SSS_LAUNCH(true, true); else SSS_LAUNCH(true, false);

@@ -1,0 +1,146 @@
+"""The set-similarity self-join pipeline on the GPU, checked against the
+oracle: seeded token sets, prefix-filter candidates (exactly the oracle's
+restated filter, and a superset of the brute-force join), and the batched
+CUDA-graph form of the pair kernel (equal to reset_sss and to the oracle's
+decisions, across replays of different sizes)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def R(cuda, libreset):
+    from reset_b200 import api
+    return api
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def _pairs(a, b):
+    return set(zip(host(a).tolist(), host(b).tolist())) if not isinstance(a, np.ndarray) \
+        else set(zip(a.tolist(), b.tolist()))
+
+
+@pytest.mark.parametrize("n,ulog,lo,hi", [(1, 4, 1, 1), (300, 8, 1, 40),
+                                          (5000, 16, 8, 300), (20000, 20, 8, 64)])
+def test_token_sets_properties(R, n, ulog, lo, hi):
+    off, tok = R.gen_token_sets(n, ulog, 1.6, lo, hi, seed=0x5EED0000 + n)
+    o, t = host(off), host(tok)
+    assert o[0] == 0 and o[-1] == t.size and o.size == n + 1
+    sz = np.diff(o)
+    assert sz.min() >= 1 and sz.max() <= hi
+    assert t.min() >= 0 and t.max() < (1 << ulog)
+    row = np.repeat(np.arange(n), sz)
+    key = row.astype(np.int64) << 32 | t
+    assert np.all(np.diff(key) > 0)             # rows sorted, no duplicates
+    off2, tok2 = R.gen_token_sets(n, ulog, 1.6, lo, hi, seed=0x5EED0000 + n)
+    assert np.array_equal(host(off2), o) and np.array_equal(host(tok2), t)
+
+
+def test_token_sets_rejects_bad_arguments(R):
+    from reset_b200._lib import ResetError
+    for args in [(0, 10, 1.5, 1, 4), (1 << 21, 10, 1.5, 1, 4), (10, 3, 1.5, 1, 4),
+                 (10, 10, 1.5, 5, 4), (10, 10, 1.5, 1, 20000)]:
+        with pytest.raises(ResetError):
+            R.gen_token_sets(*args)
+
+
+@pytest.mark.parametrize("n,ulog,lo,hi,num,den", [
+    (400, 7, 2, 30, 1, 2), (1500, 9, 4, 40, 7, 10), (1200, 8, 1, 12, 3, 4),
+    (900, 10, 10, 60, 9, 10), (60, 4, 1, 16, 1, 1)])
+def test_prefix_candidates_match_oracle(R, oracle_mod, n, ulog, lo, hi, num, den):
+    off, tok = R.gen_token_sets(n, ulog, 1.3, lo, hi, seed=0x5EED1000 + n)
+    pa, pb = R.prefix_candidates(off, tok, ulog, num, den)
+    a, b = host(pa), host(pb)
+    assert np.all(a < b)
+    k = a.astype(np.int64) << 32 | b
+    assert np.all(np.diff(k) > 0)               # distinct, sorted by (a, b)
+    oa, ob = oracle_mod.prefix_candidates(host(off), host(tok), num, den)
+    assert np.array_equal(a, oa) and np.array_equal(b, ob)
+    ja, jb = oracle_mod.jaccard_join(host(off), host(tok), num, den)
+    assert _pairs(ja, jb) <= _pairs(a, b)        # no qualifying pair is lost
+
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_self_join_pipeline_equals_brute_force(R, oracle_mod, cuda, hier):
+    torch = cuda
+    n, ulog, num, den = 1500, 9, 7, 10
+    off, tok = R.gen_token_sets(n, ulog, 1.3, 4, 40, seed=0x5EED2000)
+    t = R.Table(off, tok, hierarchical=hier)
+    pa, pb = R.prefix_candidates(off, tok, ulog, num, den)
+    batch = R.Batch(t, tok, capacity=max(1, pa.numel()), num=num, den=den)
+    flags, inter = batch(pa, pb)
+    torch.cuda.synchronize()
+    keep = host(flags).astype(bool)
+    got = _pairs(host(pa)[keep], host(pb)[keep])
+    ja, jb = oracle_mod.jaccard_join(host(off), host(tok), num, den)
+    assert got == _pairs(ja, jb)
+    assert len(got) > 0
+    batch.close()
+
+
+def test_batch_equals_sss_across_replays(R, oracle_mod, cuda):
+    torch = cuda
+    off, cols = R.gen_rmat(12, 16, 0x5EED3000, oriented=False)
+    t = R.Table(off, cols, hierarchical=True)
+    n = off.numel() - 1
+    g = torch.Generator(device="cuda").manual_seed(5)
+    cap = 200_000
+    batch = R.Batch(t, cols, capacity=cap, num=1, den=4)
+    ot = oracle_mod.Table(host(off), host(cols), hier=1)
+    for P in [cap, 1, 0, 77_777, 31, 32, 33, 150_000]:
+        pa = torch.randint(0, n, (P,), device="cuda", dtype=torch.int32, generator=g)
+        pb = torch.randint(0, n, (P,), device="cuda", dtype=torch.int32, generator=g)
+        f, i = batch(pa, pb)
+        f2, i2 = R.sss(t, off, cols, pa, pb, num=1, den=4)
+        assert torch.equal(f, f2) and torch.equal(i, i2)
+        if 0 < P <= 100_000:
+            of, oi = oracle_mod.sss(ot, host(pa), host(pb), mode=1, num=1, den=4)
+            assert np.array_equal(host(f), of.astype(np.uint8))
+            assert np.array_equal(host(i), oi)
+    t.check()
+    batch.close()
+
+
+def test_batch_replays_queue_without_host_sync(R, cuda):
+    """Back-to-back runs of different sizes on one stream, read at the end:
+    each replay sees its own pair count."""
+    torch = cuda
+    off, cols = R.gen_rmat(10, 16, 0x5EED3001, oriented=False)
+    t = R.Table(off, cols)
+    n = off.numel() - 1
+    pa = torch.randint(0, n, (5000,), device="cuda", dtype=torch.int32)
+    pb = torch.randint(0, n, (5000,), device="cuda", dtype=torch.int32)
+    want, _ = R.sss(t, off, cols, pa, pb, num=1, den=3)
+    batch = R.Batch(t, cols, capacity=5000, num=1, den=3)
+    batch.pair_a.copy_(pa)
+    batch.pair_b.copy_(pb)
+    outs = []
+    for P in [10, 5000, 2500, 4999]:
+        batch.flags.fill_(2)
+        batch.run(P)
+        outs.append(batch.flags.clone())
+    torch.cuda.synchronize()
+    for P, f in zip([10, 5000, 2500, 4999], outs):
+        assert torch.equal(f[:P], want[:P])
+        assert bool((f[P:] == 2).all())
+    batch.close()
+
+
+def test_batch_rejects_bad_sizes(R, libreset, cuda):
+    off, cols = R.gen_rmat(8, 8, 1, oriented=False)
+    t = R.Table(off, cols)
+    h = C.c_void_p()
+    assert libreset.reset_batch_create(t.handle, C.c_void_p(cols.data_ptr()), 0, 7, 10,
+                                       C.byref(h), None) == 3
+    assert libreset.reset_batch_create(t.handle, C.c_void_p(cols.data_ptr()), 1 << 31, 7, 10,
+                                       C.byref(h), None) == 3
+    batch = R.Batch(t, cols, capacity=100)
+    assert libreset.reset_batch_run(batch._h, 101, None) == 3
+    assert libreset.reset_batch_run(batch._h, -1, None) == 3
+    batch.close()

@@ -236,3 +236,23 @@ def test_relabel_spreads_hash_buckets(oracle_mod):
         occ = (t.table.reshape(t.bucket, t.bucket_num) != -1).sum(0)
         full = float((occ == t.bucket).mean())
         assert lo <= full <= hi, (relabel, full)
+
+
+def test_prefix_filter_keeps_every_join_pair(oracle_mod):
+    """The restated prefix filter loses no pair of the brute-force join."""
+    rng = np.random.default_rng(11)
+    for num, den, U in [(1, 2, 40), (7, 10, 60), (9, 10, 30), (1, 1, 20)]:
+        sizes = rng.integers(1, 15, size=150)
+        rows = [np.sort(rng.choice(U, size=min(s, U), replace=False)) for s in sizes]
+        rows += [rows[i].copy() for i in range(0, 150, 10)]   # exact duplicates: J = 1
+        off = np.zeros(len(rows) + 1, np.int32)
+        off[1:] = np.cumsum([r.size for r in rows])
+        tok = np.concatenate(rows).astype(np.int32)
+        ja, jb = oracle_mod.jaccard_join(off, tok, num, den)
+        ca, cb = oracle_mod.prefix_candidates(off, tok, num, den)
+        assert set(zip(ja.tolist(), jb.tolist())) <= set(zip(ca.tolist(), cb.tolist()))
+        assert ja.size > 0
+        # the join's rule, checked pair by pair in Python for a few pairs
+        for a, b in list(zip(ja.tolist(), jb.tolist()))[:20]:
+            A, B = set(rows[a].tolist()), set(rows[b].tolist())
+            assert den * len(A & B) >= num * len(A | B)
