@@ -1,0 +1,74 @@
+#!/usr/bin/env python
+"""Time the reference's own triangle-count kernel (oracle/_ref/ref_tc: the
+reference's triangle-count/TC.cu + hashtable.cu compiled unchanged for
+sm_100a) on the same seeded R-MAT graph bench.py uses, for a side-by-side
+with this library's kernel on the same GPU.  Test/measurement
+infrastructure: the graph comes from the CPU oracle's generator (identical
+to the device generator), is written in the reference's TC input format
+(triangle-count/TC.cu:236-245) to a scratch folder, and ref_tc prints the
+kernel time of dynamic_triangle_count (TC.cu:128-190, launch shape of
+TC.cu:268-275) in both hash modes, timed with CUDA events.
+
+    python oracle/ref_bench.py --scale 22 [--workdir DIR]
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+
+def write_arr(path, a):
+    with open(path, "wb") as f:
+        np.array([a.size], np.uint64).tofile(f)
+        np.ascontiguousarray(a).tofile(f)
+
+
+def write_int(path, x):
+    np.array([x], np.int32).tofile(path)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--seed", type=lambda s: int(s, 0), default=0x5EED0024)
+    ap.add_argument("--workdir", default=None)
+    a = ap.parse_args()
+    import oracle
+    seed = a.seed
+    exe = os.path.join(HERE, "_ref", "ref_tc")
+    if not os.path.exists(exe):
+        sys.exit("oracle/_ref/ref_tc is missing (build it with `make -C oracle ref`)")
+    t0 = time.perf_counter()
+    off, cols = oracle.rmat_graph(a.scale, a.edge_factor, seed, oriented=True)
+    gen = time.perf_counter() - t0
+    work = a.workdir or tempfile.mkdtemp(prefix="reset_ref_tc_")
+    ind, outd = os.path.join(work, "in"), os.path.join(work, "out")
+    os.makedirs(ind, exist_ok=True)
+    os.makedirs(outd, exist_ok=True)
+    try:
+        write_arr(os.path.join(ind, "csr_offsets_tri.bin"), off.astype(np.int32))
+        write_arr(os.path.join(ind, "csr_cols_tri.bin"), cols.astype(np.int32))
+        write_int(os.path.join(ind, "num_nodes_tri.bin"), off.size - 1)
+        write_int(os.path.join(ind, "num_edges_tri.bin"), cols.size)
+        print(f"graph: scale {a.scale} seed {seed:#x} n={off.size - 1} m={cols.size} "
+              f"(CPU generator {gen:.1f} s)", flush=True)
+        r = subprocess.run([exe, ind, outd], capture_output=True, text=True)
+        print(r.stdout.strip())
+        if r.returncode != 0:
+            print(r.stderr.strip(), file=sys.stderr)
+        return r.returncode
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
