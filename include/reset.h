@@ -278,6 +278,99 @@ reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2, double size_
                                   int64_t *m_out, reset_stream_t stream);
 reset_status reset_free(void *d_ptr);
 
+/* ---- served form ----------------------------------------------------------- */
+
+/* A request loop over device-resident indexes with continuous batching: a
+ * scheduler thread drains the arrival queue into batches whenever one of
+ * `streams` slots is free, admitting requests (FIFO) while their device bytes
+ * fit the memory budget; batches on different slots overlap on the GPU.  A
+ * result depends only on its request and the index: it is the same whether
+ * the request ran alone or in a mix.  No counterpart in the reference (its
+ * applications run one offline batch per process: triangle-count/TC.cu:
+ * 192-247, set-similarity-search/sss.cu:191-244,
+ * information-retrieval/ir.cu:213-267, set_size/intersection.cu:183-192). */
+typedef struct reset_server reset_server;
+
+typedef struct {
+  int32_t streams;            /* batches in flight at once (default 4)        */
+  int32_t max_batch_requests; /* requests per batch at most (default 1024)    */
+  int64_t mem_budget_bytes;   /* device bytes for batches; 0 = half the free
+                                 device memory when the server starts        */
+  int32_t reserved[8];
+} reset_server_config;
+
+enum {
+  RESET_REQ_IR = 1,        /* args: query terms (first term's list filtered
+                              by the others, as reset_ir); -> docs          */
+  RESET_REQ_PAIRS = 2,     /* args: (a, b) set pairs; num/den threshold;
+                              -> values = |A ∩ B|, flags, count = #similar  */
+  RESET_REQ_TRIPLES = 3,   /* args: (a, b, c); -> values = |A ∩ B ∩ C|       */
+  RESET_REQ_TC_VERTEX = 4, /* args: vertices v of an oriented graph index;
+                              -> values = sum over w in N(v) of
+                                 |N(v) ∩ N(w)| (triangles with v first)     */
+  RESET_REQ_RAW = 5        /* args: A, args2: B (host keys >= 0, no index);
+                              -> count = |A ∩ B| with A's multiplicity       */
+};
+
+typedef struct {
+  int32_t kind;        /* RESET_REQ_*                                        */
+  int32_t index;       /* from reset_server_add_index (unused by RAW)        */
+  const int32_t *args; /* host array, copied at submit                       */
+  int64_t nargs;
+  const int32_t *args2;
+  int64_t nargs2;
+  int32_t num, den;    /* PAIRS: similar iff den*I >= num*U, U > 0           */
+  int64_t arrival_ns;  /* reset_now_ns() clock; 0 = the submit time          */
+  int32_t reserved[4];
+} reset_request;
+
+typedef struct {
+  reset_status status;
+  int32_t kind;
+  int64_t count;          /* IR: #docs; PAIRS: #similar; others: sum        */
+  const int32_t *docs;    /* IR result list (ndocs), first-term order       */
+  int64_t ndocs;
+  const int64_t *values;  /* per pair / triple / vertex (nvalues)           */
+  int64_t nvalues;
+  const uint8_t *flags;   /* PAIRS decisions (nvalues)                      */
+  double queue_us;        /* arrival -> batch launch                        */
+  double service_us;      /* batch launch -> results on the host            */
+  double latency_us;      /* arrival -> results on the host                 */
+  int64_t batch_id;
+  int32_t batch_size;
+  int32_t reserved;
+} reset_result;
+
+typedef struct {
+  int64_t completed, batches, max_batch, pending;
+  int64_t inflight_batches, max_inflight_batches;
+  int64_t budget_bytes, in_use_bytes, max_in_use_bytes;
+  double mean_batch;
+  int64_t reserved[4];
+} reset_server_counters;
+
+void reset_server_config_default(reset_server_config *cfg);
+int64_t reset_now_ns(void);
+reset_status reset_server_create(const reset_server_config *cfg, reset_server **out);
+/* Registers a built table as an index; d_off must be the offsets it was
+ * built on (their host copy is taken for planning).  The table and arrays
+ * must outlive the server. */
+reset_status reset_server_add_index(reset_server *s, const reset_table *t,
+                                    const int32_t *d_off, const int32_t *d_elems,
+                                    int32_t *index_out);
+/* Queues a request; invalid ids fail here (RESET_ERR_ARG).  A request that
+ * can never fit the memory budget completes with RESET_ERR_OOM. */
+reset_status reset_server_submit(reset_server *s, const reset_request *req,
+                                 uint64_t *ticket);
+/* Waits up to timeout_ms (< 0: no limit; RESET_ERR_TIMEOUT when it runs
+ * out).  The result's arrays stay valid until reset_server_release. */
+reset_status reset_server_wait(reset_server *s, uint64_t ticket, int32_t timeout_ms,
+                               reset_result *out);
+reset_status reset_server_release(reset_server *s, uint64_t ticket);
+reset_status reset_server_stats(reset_server *s, reset_server_counters *out);
+/* Finishes queued requests, then stops. */
+reset_status reset_server_destroy(reset_server *s);
+
 /* ---- tuning --------------------------------------------------------------- */
 
 /* Process-wide kernel knobs (no counterpart in the reference, whose launch

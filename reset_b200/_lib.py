@@ -43,6 +43,38 @@ class TableView(C.Structure):
                 ("d_off", C.c_void_p)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("streams", C.c_int32), ("max_batch_requests", C.c_int32),
+                ("mem_budget_bytes", C.c_int64), ("reserved", C.c_int32 * 8)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("index", C.c_int32),
+                ("args", C.POINTER(C.c_int32)), ("nargs", C.c_int64),
+                ("args2", C.POINTER(C.c_int32)), ("nargs2", C.c_int64),
+                ("num", C.c_int32), ("den", C.c_int32), ("arrival_ns", C.c_int64),
+                ("reserved", C.c_int32 * 4)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int32), ("kind", C.c_int32), ("count", C.c_int64),
+                ("docs", C.POINTER(C.c_int32)), ("ndocs", C.c_int64),
+                ("values", C.POINTER(C.c_int64)), ("nvalues", C.c_int64),
+                ("flags", C.POINTER(C.c_uint8)), ("queue_us", C.c_double),
+                ("service_us", C.c_double), ("latency_us", C.c_double),
+                ("batch_id", C.c_int64), ("batch_size", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("batches", C.c_int64),
+                ("max_batch", C.c_int64), ("pending", C.c_int64),
+                ("inflight_batches", C.c_int64), ("max_inflight_batches", C.c_int64),
+                ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64),
+                ("max_in_use_bytes", C.c_int64), ("mean_batch", C.c_double),
+                ("reserved", C.c_int64 * 4)]
+
+
 P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
@@ -76,6 +108,15 @@ SIGNATURES = {
                                    C.POINTER(P), C.POINTER(P), C.POINTER(I64), P]),
     "reset_prefix_candidates": (I32, [P, P, I32, I64, I32, I32, I32, C.POINTER(P),
                                       C.POINTER(P), C.POINTER(I64), P]),
+    "reset_server_config_default": (None, [C.POINTER(ServerConfig)]),
+    "reset_now_ns": (I64, []),
+    "reset_server_create": (I32, [C.POINTER(ServerConfig), C.POINTER(P)]),
+    "reset_server_add_index": (I32, [P, P, P, P, C.POINTER(I32)]),
+    "reset_server_submit": (I32, [P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "reset_server_wait": (I32, [P, C.c_uint64, I32, C.POINTER(Result)]),
+    "reset_server_release": (I32, [P, C.c_uint64]),
+    "reset_server_stats": (I32, [P, C.POINTER(ServerCounters)]),
+    "reset_server_destroy": (I32, [P]),
     "reset_free": (I32, [P]),
     "reset_last_error_string": (C.c_char_p, []),
     "reset_status_string": (C.c_char_p, [I32]),

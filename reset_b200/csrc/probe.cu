@@ -413,6 +413,41 @@ reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
   return RESET_OK;
 }
 
+int ir_slice_size() { return kIrSlice; }
+
+// Conjunctive retrieval for a batch whose slice plan was made by the caller:
+// sl_off[q] = sum over earlier queries of ceil(df(first term) / kIrSlice),
+// sl_off[nq] = total_slices; res_off as for reset_ir.  Uses the table's own
+// descriptors (the index CSR it was built on).  No allocation and no
+// synchronisation: sl_cnt (total_slices ints) is caller scratch.
+reset_status ir_launch_planned(const reset_table* t, const int32_t* docs,
+                               const int32_t* query, const int32_t* qoff,
+                               int32_t nq, const int64_t* sl_off,
+                               int64_t total_slices, const int64_t* res_off,
+                               int32_t* res, int32_t* sl_cnt, int32_t* cnt,
+                               cudaStream_t st) {
+  if (nq <= 0) return RESET_OK;
+  if (total_slices > 0) {
+#define IR_P(H)                                                                \
+    do {                                                                       \
+      const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,       \
+                                   persistent_grid((const void*)ir_slice_kernel<H>)); \
+      note_launch();                                                           \
+      ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
+          t->d_desc, t->n, docs, query, qoff, nq, sl_off, res_off, res, sl_cnt, \
+          t->d_table, t->bucket_num, t->bucket, t->lg_max, t->d_status);       \
+    } while (0)
+    if (t->hier) IR_P(true); else IR_P(false);
+#undef IR_P
+    RST_CUDA(cudaGetLastError());
+  }
+  note_launch();
+  ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8),
+                      kThreads, 0, st>>>(sl_off, nq, res_off, res, sl_cnt, cnt);
+  RST_CUDA(cudaGetLastError());
+  return RESET_OK;
+}
+
 }  // namespace rst
 
 using namespace rst;
