@@ -276,6 +276,15 @@ reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2, double size_
                                   int32_t size_lo, int32_t size_hi, uint64_t seed,
                                   int32_t **d_off_out, int32_t **d_tokens_out,
                                   int64_t *m_out, reset_stream_t stream);
+/* Seeded inverted index (stand-in for the IR corpora): term t (0-based
+ * rank) gets df(t) = clamp(round(df_max * (t+1)^-zipf_s), 1, ndocs) uniform
+ * doc-id draws from [0, ndocs); duplicates removed, posting lists sorted.
+ * Outputs (d_toff[nterms+1], d_docs[m]) allocated with cudaMalloc, owned by
+ * the caller.  Synchronises `stream`. */
+reset_status reset_gen_inverted_index(int32_t nterms, int32_t ndocs, double zipf_s,
+                                      int64_t df_max, uint64_t seed,
+                                      int32_t **d_toff_out, int32_t **d_docs_out,
+                                      int64_t *m_out, reset_stream_t stream);
 reset_status reset_free(void *d_ptr);
 
 /* ---- served form ----------------------------------------------------------- */

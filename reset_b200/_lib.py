@@ -108,6 +108,8 @@ SIGNATURES = {
                                    C.POINTER(P), C.POINTER(P), C.POINTER(I64), P]),
     "reset_prefix_candidates": (I32, [P, P, I32, I64, I32, I32, I32, C.POINTER(P),
                                       C.POINTER(P), C.POINTER(I64), P]),
+    "reset_gen_inverted_index": (I32, [I32, I32, C.c_double, I64, C.c_uint64,
+                                       C.POINTER(P), C.POINTER(P), C.POINTER(I64), P]),
     "reset_server_config_default": (None, [C.POINTER(ServerConfig)]),
     "reset_now_ns": (I64, []),
     "reset_server_create": (I32, [C.POINTER(ServerConfig), C.POINTER(P)]),

@@ -316,6 +316,24 @@ def gen_token_sets(n: int, universe_log2: int = 20, size_s: float = 1.6,
     return off, tok
 
 
+def gen_inverted_index(nterms: int, ndocs: int, zipf_s: float = 1.1,
+                       df_max: Optional[int] = None, seed: int = 0x5EED0044, stream=None):
+    """Seeded inverted index on the device -> (toff int32[nterms+1], docs int32)."""
+    L = _lib()
+    df_max = ndocs // 2 if df_max is None else df_max
+    po, pd, m = C.c_void_p(), C.c_void_p(), C.c_int64()
+    check(L.reset_gen_inverted_index(nterms, ndocs, zipf_s, df_max, seed, C.byref(po),
+                                     C.byref(pd), C.byref(m), _stream(stream)))
+    try:
+        toff = _view(po.value, nterms + 1, torch.int32).clone()
+        docs = _view(pd.value, m.value, torch.int32).clone()
+        torch.cuda.current_stream().synchronize()
+    finally:
+        L.reset_free(po)
+        L.reset_free(pd)
+    return toff, docs
+
+
 def prefix_candidates(off: torch.Tensor, tokens: torch.Tensor, universe_log2: int,
                       num: int = 7, den: int = 10, stream=None):
     """Prefix-filter candidate pairs (a < b, sorted) -> (pa, pb) int32."""

@@ -218,6 +218,24 @@ __global__ void pair_split_kernel(const uint64_t* __restrict__ pairs, int64_t np
   }
 }
 
+// Inverted index: draw j of term t is a uniform doc id; term t's draws sit
+// at doff[t] .. doff[t+1] (flat over all draws, owner by binary search).
+__global__ void draw_postings_kernel(const int64_t* __restrict__ doff, int32_t nterms,
+                                     int64_t ndraw, int32_t ndocs, int dbits,
+                                     uint64_t seed, uint64_t* __restrict__ keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ndraw;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nterms - 1;  // largest t with doff[t] <= i
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (doff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    uint64_t d = (uint64_t)(unif(seed, (uint64_t)lo, (uint64_t)(i - doff[lo])) * ndocs);
+    if (d >= (uint64_t)ndocs) d = ndocs - 1;
+    keys[i] = ((uint64_t)lo << dbits) | d;
+  }
+}
+
 int g_grid(int64_t items) {
   int64_t g = (items + 255) / 256, cap = (int64_t)sm_count() * 16;
   return (int)(g < 1 ? 1 : (g > cap ? cap : g));
@@ -449,5 +467,85 @@ extern "C" reset_status reset_prefix_candidates(const int32_t* d_off,
   *d_pa_out = pa;
   *d_pb_out = pbb;
   *np_out = np;
+  return RESET_OK;
+}
+
+extern "C" reset_status reset_gen_inverted_index(int32_t nterms, int32_t ndocs,
+                                                 double zipf_s, int64_t df_max,
+                                                 uint64_t seed, int32_t** d_toff_out,
+                                                 int32_t** d_docs_out, int64_t* m_out,
+                                                 reset_stream_t stream) {
+  if (!d_toff_out || !d_docs_out || !m_out) return arg_fail("NULL output");
+  if (nterms < 1 || nterms > (1 << 26)) return arg_fail("nterms must be in 1..2^26");
+  if (ndocs < 1) return arg_fail("ndocs must be >= 1");
+  if (df_max < 1) return arg_fail("df_max must be >= 1");
+  if (!(zipf_s >= 0.0)) return arg_fail("zipf_s must be >= 0");
+  int dbits = 1;
+  while ((1ll << dbits) < ndocs) ++dbits;
+  int tbits = 1;
+  while ((1ll << tbits) < nterms) ++tbits;
+  if (dbits + tbits > 64) return arg_fail("too many terms x docs");
+  cudaStream_t st = as_stream(stream);
+  std::vector<int64_t> doff((size_t)nterms + 1);
+  int64_t tot = 0;
+  for (int32_t t = 0; t < nterms; ++t) {
+    doff[t] = tot;
+    int64_t df = (int64_t)std::llround((double)df_max * std::pow((double)(t + 1), -zipf_s));
+    if (df < 1) df = 1;
+    if (df > ndocs) df = ndocs;
+    tot += df;
+  }
+  doff[nterms] = tot;
+  if (tot > INT32_MAX) return arg_fail("more than 2^31 postings");
+  Temps tmp(st);
+  int64_t* d_doff;
+  uint64_t *k0, *k1;
+  int64_t* d_nu;
+  RST_CUDA(tmp.get(&d_doff, sizeof(int64_t) * (nterms + 1)));
+  RST_CUDA(tmp.get(&k0, sizeof(uint64_t) * tot));
+  RST_CUDA(tmp.get(&k1, sizeof(uint64_t) * tot));
+  RST_CUDA(tmp.get(&d_nu, sizeof(int64_t)));
+  RST_CUDA(cudaMemcpyAsync(d_doff, doff.data(), sizeof(int64_t) * (nterms + 1),
+                           cudaMemcpyHostToDevice, st));
+  note_launch();
+  draw_postings_kernel<<<g_grid(tot), 256, 0, st>>>(d_doff, nterms, tot, ndocs, dbits,
+                                                   seed, k0);
+  RST_CUDA(cudaGetLastError());
+  cub::DoubleBuffer<uint64_t> db(k0, k1);
+  size_t ts = 0, tu = 0;
+  RST_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, ts, db, tot, 0, dbits + tbits, st));
+  RST_CUDA(cub::DeviceSelect::Unique(nullptr, tu, k0, k1, d_nu, tot, st));
+  void* d_ts;
+  RST_CUDA(tmp.get(&d_ts, ts > tu ? ts : tu));
+  RST_CUDA(cub::DeviceRadixSort::SortKeys(d_ts, ts, db, tot, 0, dbits + tbits, st));
+  RST_CUDA(cub::DeviceSelect::Unique(d_ts, tu, db.Current(), db.Alternate(), d_nu, tot, st));
+  int64_t m = 0;
+  RST_CUDA(cudaMemcpyAsync(&m, d_nu, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  RST_CUDA(cudaStreamSynchronize(st));
+  int32_t *toff = nullptr, *docs = nullptr, *cnt;
+  RST_CUDA(tmp.get(&cnt, sizeof(int32_t) * (nterms + 1)));
+  RST_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (nterms + 1), st));
+  RST_CUDA(cudaMalloc(&toff, sizeof(int32_t) * (nterms + 1)));
+  cudaError_t e = cudaMalloc(&docs, sizeof(int32_t) * (m > 0 ? m : 1));
+  if (e != cudaSuccess) {
+    cudaFree(toff);
+    return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+  }
+  note_launch();
+  split_keys_kernel<<<g_grid(m), 256, 0, st>>>(db.Alternate(), m, dbits, docs, cnt);
+  size_t tb2 = 0;
+  e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, cnt, toff, nterms + 1, st);
+  void* d_tb2 = nullptr;
+  if (e == cudaSuccess) e = tmp.get(&d_tb2, tb2);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(d_tb2, tb2, cnt, toff, nterms + 1, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaFree(toff);
+    cudaFree(docs);
+    return cuda_fail(e, "inverted index", __FILE__, __LINE__);
+  }
+  *d_toff_out = toff;
+  *d_docs_out = docs;
+  *m_out = m;
   return RESET_OK;
 }
