@@ -62,6 +62,25 @@ def parse():
     ap.add_argument("--warp-pair-min", type=int, default=0)
     ap.add_argument("--tc-method", type=int, default=0, choices=[0, 1, 2],
                     help="0 default (edge-flattened), 1 edge-flattened, 2 vertex-staged")
+    ap.add_argument("--workload", default="tc",
+                    choices=["tc", "sss-join", "ir-serve", "mixed-serve"],
+                    help="tc: TC on R-MAT (default); sss-join: batched Jaccard self-join; "
+                         "ir-serve: served conjunctive IR; mixed-serve: served mixed "
+                         "intersections on R-MAT scale 22")
+    # sss-join
+    ap.add_argument("--sets", type=int, default=2_000_000)
+    ap.add_argument("--size-hi", type=int, default=1024)
+    ap.add_argument("--dup-frac", type=float, default=0.2)
+    # serving
+    ap.add_argument("--terms", type=int, default=1_000_000)
+    ap.add_argument("--docs", type=int, default=20_000_000)
+    ap.add_argument("--df-max", type=int, default=10_000_000)
+    ap.add_argument("--requests", type=int, default=20000,
+                    help="requests in the capacity burst of a serving workload")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="length of each Poisson arrival phase")
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--max-batch", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -362,6 +381,13 @@ def run_reference(a, rank, world):
 def main():
     a = parse()
     rank, world, local = dist_env()
+    if a.workload != "tc":
+        import bench_serving
+        if a.impl == "reference":
+            bench_serving.run_reference(a, rank, world)
+        else:
+            bench_serving.run_ours(a, rank, world, local)
+        return
     if a.impl == "reference":
         run_reference(a, rank, world)
     else:

@@ -269,11 +269,15 @@ reset_status reset_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed,
 /* Seeded token sets (stand-in for the set-similarity datasets): n sets,
  * set sizes Zipf(size_s) on [size_lo, size_hi], tokens drawn from a
  * Zipf(1)-like law over 2^universe_log2 ranks and relabeled by a seeded
- * bijection; duplicates removed, rows sorted.  Outputs allocated with
- * cudaMalloc, owned by the caller.  n < 2^21, size_hi <= 16384,
- * universe_log2 in 4..24.  Synchronises `stream`. */
+ * bijection; duplicates removed, rows sorted.  With probability dup_frac a
+ * set (other than the first) is a near-duplicate of the nearest earlier
+ * non-duplicate set within 256: same size, each of that set's draws kept
+ * with probability keep ~ U(keep_min, 1), fresh draws otherwise.  Outputs
+ * allocated with cudaMalloc, owned by the caller.  n < 2^21,
+ * size_hi <= 16384, universe_log2 in 4..24.  Synchronises `stream`. */
 reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2, double size_s,
-                                  int32_t size_lo, int32_t size_hi, uint64_t seed,
+                                  int32_t size_lo, int32_t size_hi, double dup_frac,
+                                  double keep_min, uint64_t seed,
                                   int32_t **d_off_out, int32_t **d_tokens_out,
                                   int64_t *m_out, reset_stream_t stream);
 /* Seeded inverted index (stand-in for the IR corpora): term t (0-based
@@ -355,7 +359,10 @@ typedef struct {
   int64_t inflight_batches, max_inflight_batches;
   int64_t budget_bytes, in_use_bytes, max_in_use_bytes;
   double mean_batch;
-  int64_t reserved[4];
+  double launch_host_us;  /* host time spent packing and launching batches  */
+  double batch_us;        /* sum over batches of launch -> results unpacked */
+  int64_t arena_bytes;    /* device buffers the slots keep for reuse        */
+  int64_t reserved[1];
 } reset_server_counters;
 
 void reset_server_config_default(reset_server_config *cfg);

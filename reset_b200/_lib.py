@@ -72,7 +72,8 @@ class ServerCounters(C.Structure):
                 ("inflight_batches", C.c_int64), ("max_inflight_batches", C.c_int64),
                 ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64),
                 ("max_in_use_bytes", C.c_int64), ("mean_batch", C.c_double),
-                ("reserved", C.c_int64 * 4)]
+                ("launch_host_us", C.c_double), ("batch_us", C.c_double),
+                ("arena_bytes", C.c_int64), ("reserved", C.c_int64 * 1)]
 
 
 P = C.c_void_p
@@ -104,7 +105,8 @@ SIGNATURES = {
                                   C.POINTER(P)]),
     "reset_batch_run": (I32, [P, I64, P]),
     "reset_batch_destroy": (I32, [P]),
-    "reset_gen_token_sets": (I32, [I32, I32, C.c_double, I32, I32, C.c_uint64,
+    "reset_gen_token_sets": (I32, [I32, I32, C.c_double, I32, I32, C.c_double,
+                                   C.c_double, C.c_uint64,
                                    C.POINTER(P), C.POINTER(P), C.POINTER(I64), P]),
     "reset_prefix_candidates": (I32, [P, P, I32, I64, I32, I32, I32, C.POINTER(P),
                                       C.POINTER(P), C.POINTER(I64), P]),

@@ -300,11 +300,13 @@ class Batch:
 
 def gen_token_sets(n: int, universe_log2: int = 20, size_s: float = 1.6,
                    size_lo: int = 8, size_hi: int = 512, seed: int = 0x5EED0033,
-                   stream=None):
-    """Seeded token sets on the device -> (off int32[n+1], tokens int32)."""
+                   dup_frac: float = 0.0, keep_min: float = 0.8, stream=None):
+    """Seeded token sets on the device -> (off int32[n+1], tokens int32);
+    dup_frac of them planted near-duplicates (see reset_gen_token_sets)."""
     L = _lib()
     po, pt, m = C.c_void_p(), C.c_void_p(), C.c_int64()
-    check(L.reset_gen_token_sets(n, universe_log2, size_s, size_lo, size_hi, seed,
+    check(L.reset_gen_token_sets(n, universe_log2, size_s, size_lo, size_hi, dup_frac,
+                                 keep_min, seed,
                                  C.byref(po), C.byref(pt), C.byref(m), _stream(stream)))
     try:
         off = _view(po.value, n + 1, torch.int32).clone()

@@ -261,7 +261,8 @@ __global__ void ir_total_kernel(const int64_t* __restrict__ ns_excl,
 // One warp per slice of kIrSlice candidates of the first term's list:
 // every candidate is checked against all further terms (early exit per
 // lane), survivors are compacted with ballot/popc to the front of the
-// slice's own region of the result buffer, in first-term order.
+// slice's own region stage[slice * kIrSlice ...], in first-term order, and
+// their number goes to sl_cnt[slice].
 template <bool HIER>
 __global__ void __launch_bounds__(kThreads)
     ir_slice_kernel(const int4* __restrict__ desc, int32_t n,
@@ -269,8 +270,7 @@ __global__ void __launch_bounds__(kThreads)
                     const int32_t* __restrict__ query,
                     const int32_t* __restrict__ qoff, int32_t nq,
                     const int64_t* __restrict__ sl_off,
-                    const int64_t* __restrict__ res_off,
-                    int32_t* __restrict__ res, int32_t* __restrict__ sl_cnt,
+                    int32_t* __restrict__ stage, int32_t* __restrict__ sl_cnt,
                     const int32_t* __restrict__ table, int64_t bn, int b,
                     int lg_max, int32_t* __restrict__ status) {
   const int lane = threadIdx.x & 31;
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kThreads)
     const int4 d0 = desc[query[qs]];
     const int64_t j0 = (sidx - sl_off[q]) * kIrSlice;
     const int64_t j1 = min((int64_t)d0.y, j0 + kIrSlice);
-    int32_t* out = res + res_off[q] + j0;
+    int32_t* out = stage + sidx * kIrSlice;
     int w = 0;
     for (int64_t jb = j0; jb < j1; jb += 32) {
       const int64_t j = jb + lane;
@@ -318,37 +318,103 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// One warp per query: slides the survivors of slices 1.. down behind those
-// of slice 0 (destination never past the source) and writes the count.
+// Exclusive scan of per-slice survivor counts in one block (chunks of
+// blockDim with a running carry): pos[s] = survivors before slice s,
+// pos[ns] = all survivors.
+__global__ void slice_scan_kernel(const int32_t* __restrict__ cnt, int64_t ns,
+                                  int64_t* __restrict__ pos) {
+  __shared__ int64_t s_part[32];
+  __shared__ int64_t s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < ns; base += blockDim.x) {
+    const int64_t i = base + tid;
+    const int64_t v = i < ns ? cnt[i] : 0;
+    int64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_part[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      int64_t w = lane < nw ? s_part[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t t = __shfl_up_sync(kFull, w, o);
+        if (lane >= o) w += t;
+      }
+      if (lane < nw) s_part[lane] = w;
+    }
+    __syncthreads();
+    const int64_t before = s_carry + (warp > 0 ? s_part[warp - 1] : 0);
+    if (i < ns) pos[i] = before + incl - v;
+    __syncthreads();
+    if (tid == blockDim.x - 1) s_carry = before + incl;
+    __syncthreads();
+  }
+  if (tid == 0) pos[ns] = s_carry;
+}
+
+// One warp per slice: copies its survivors out of the stage, out of place,
+// so all slices move in parallel.  Query q's survivors land at
+//   res + res_off[q] + (pos[s] - pos[sl_off[q]])   (res_off given), or
+//   res + pos[s]                                    (packed, res_off NULL).
 __global__ void __launch_bounds__(kThreads)
-    ir_compact_kernel(const int64_t* __restrict__ sl_off, int32_t nq,
-                      const int64_t* __restrict__ res_off,
-                      int32_t* __restrict__ res,
-                      const int32_t* __restrict__ sl_cnt,
-                      int32_t* __restrict__ cnt) {
+    ir_gather_kernel(const int64_t* __restrict__ sl_off, int32_t nq,
+                     const int32_t* __restrict__ sl_cnt,
+                     const int64_t* __restrict__ pos,
+                     const int32_t* __restrict__ stage,
+                     const int64_t* __restrict__ res_off,
+                     int32_t* __restrict__ res) {
   const int lane = threadIdx.x & 31;
+  const int64_t total = sl_off[nq];
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t q = gw; q < nq; q += nw) {
-    const int64_t s0 = sl_off[q], ns = sl_off[q + 1] - s0;
-    int32_t* base = res + res_off[q];
-    int64_t tot = ns > 0 ? sl_cnt[s0] : 0;
-    for (int64_t i = 1; i < ns; ++i) {
-      const int c = sl_cnt[s0 + i];
-      const int32_t* src = base + i * kIrSlice;
-      int32_t* dst = base + tot;
-      for (int j = 0; j < c; j += 32) {
-        int v = 0;
-        if (j + lane < c) v = src[j + lane];
-        __syncwarp();
-        if (j + lane < c) dst[j + lane] = v;
-        __syncwarp();
+  for (int64_t s = gw; s < total; s += nw) {
+    const int c = sl_cnt[s];
+    if (c == 0) continue;
+    int64_t dst = pos[s];
+    if (res_off) {
+      int lo = 0, hi = nq - 1;  // query owning slice s
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sl_off[mid] <= s) lo = mid; else hi = mid - 1;
       }
-      tot += c;
+      dst = res_off[lo] + (pos[s] - pos[sl_off[lo]]);
     }
-    if (lane == 0) cnt[q] = (int32_t)tot;
+    const int32_t* src = stage + s * kIrSlice;
+    for (int j = lane; j < c; j += 32) res[dst + j] = src[j];
   }
 }
+
+// Per query: its count, and (packed mode) where its survivors start.
+__global__ void ir_counts_kernel(const int64_t* __restrict__ sl_off, int32_t nq,
+                                 const int64_t* __restrict__ pos,
+                                 int32_t* __restrict__ cnt,
+                                 int64_t* __restrict__ packed_off) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = pos[sl_off[q]], b = pos[sl_off[q + 1]];
+    cnt[q] = (int32_t)(b - a);
+    if (packed_off) {
+      packed_off[q] = a;
+      if (q == nq - 1) packed_off[nq] = b;
+    }
+  }
+}
+
+// Launches the slice, scan, gather and count kernels for a planned batch.
+template <bool HIER>
+reset_status ir_run(const reset_table* t, const int4* desc, const int32_t* docs,
+                    const int32_t* query, const int32_t* qoff, int32_t nq,
+                    const int64_t* sl_off, int64_t total_slices,
+                    const int64_t* res_off, int32_t* res, int32_t* stage,
+                    int32_t* sl_cnt, int64_t* pos, int32_t* cnt,
+                    int64_t* packed_off, cudaStream_t st);
 
 int persistent_grid(const void* kernel) {
   int per_sm = 0;
@@ -360,6 +426,40 @@ int persistent_grid(const void* kernel) {
 int64_t clamp_grid(int64_t want, int cap) {
   if (want < 1) want = 1;
   return want < cap ? want : cap;
+}
+
+template <bool HIER>
+reset_status ir_run(const reset_table* t, const int4* desc, const int32_t* docs,
+                    const int32_t* query, const int32_t* qoff, int32_t nq,
+                    const int64_t* sl_off, int64_t total_slices,
+                    const int64_t* res_off, int32_t* res, int32_t* stage,
+                    int32_t* sl_cnt, int64_t* pos, int32_t* cnt,
+                    int64_t* packed_off, cudaStream_t st) {
+  if (total_slices > 0) {
+    const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,
+                                 persistent_grid((const void*)ir_slice_kernel<HIER>));
+    note_launch();
+    ir_slice_kernel<HIER><<<(int)g, kThreads, 0, st>>>(
+        desc, t->n, docs, query, qoff, nq, sl_off, stage, sl_cnt, t->d_table,
+        t->bucket_num, t->bucket, t->lg_max, t->d_status);
+    RST_CUDA(cudaGetLastError());
+  }
+  note_launch();
+  slice_scan_kernel<<<1, 1024, 0, st>>>(sl_cnt, total_slices, pos);
+  RST_CUDA(cudaGetLastError());
+  if (total_slices > 0) {
+    const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,
+                                 persistent_grid((const void*)ir_gather_kernel));
+    note_launch();
+    ir_gather_kernel<<<(int)g, kThreads, 0, st>>>(sl_off, nq, sl_cnt, pos, stage, res_off,
+                                                   res);
+    RST_CUDA(cudaGetLastError());
+  }
+  note_launch();
+  ir_counts_kernel<<<(int)clamp_grid((nq + 255) / 256, sm_count() * 8), 256, 0, st>>>(
+      sl_off, nq, pos, cnt, packed_off);
+  RST_CUDA(cudaGetLastError());
+  return RESET_OK;
 }
 
 // Resolves the descriptor array for a probe call: the table's own when the
@@ -415,37 +515,26 @@ reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
 
 int ir_slice_size() { return kIrSlice; }
 
-// Conjunctive retrieval for a batch whose slice plan was made by the caller:
+// Conjunctive retrieval for a batch whose slice plan is on the device:
 // sl_off[q] = sum over earlier queries of ceil(df(first term) / kIrSlice),
-// sl_off[nq] = total_slices; res_off as for reset_ir.  Uses the table's own
-// descriptors (the index CSR it was built on).  No allocation and no
-// synchronisation: sl_cnt (total_slices ints) is caller scratch.
+// sl_off[nq] = total_slices.  Scratch: stage (total_slices * kIrSlice ints),
+// sl_cnt (total_slices ints), pos (total_slices + 1 int64).  Results go to
+// res at res_off[q] (as reset_ir) or, with res_off NULL, packed query after
+// query with packed_off[q] (nq + 1 int64) giving where each starts.  Uses
+// the table's own descriptors.  No allocation, no synchronisation.
 reset_status ir_launch_planned(const reset_table* t, const int32_t* docs,
                                const int32_t* query, const int32_t* qoff,
                                int32_t nq, const int64_t* sl_off,
                                int64_t total_slices, const int64_t* res_off,
-                               int32_t* res, int32_t* sl_cnt, int32_t* cnt,
+                               int32_t* res, int32_t* stage, int32_t* sl_cnt,
+                               int64_t* pos, int32_t* cnt, int64_t* packed_off,
                                cudaStream_t st) {
   if (nq <= 0) return RESET_OK;
-  if (total_slices > 0) {
-#define IR_P(H)                                                                \
-    do {                                                                       \
-      const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,       \
-                                   persistent_grid((const void*)ir_slice_kernel<H>)); \
-      note_launch();                                                           \
-      ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
-          t->d_desc, t->n, docs, query, qoff, nq, sl_off, res_off, res, sl_cnt, \
-          t->d_table, t->bucket_num, t->bucket, t->lg_max, t->d_status);       \
-    } while (0)
-    if (t->hier) IR_P(true); else IR_P(false);
-#undef IR_P
-    RST_CUDA(cudaGetLastError());
-  }
-  note_launch();
-  ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8),
-                      kThreads, 0, st>>>(sl_off, nq, res_off, res, sl_cnt, cnt);
-  RST_CUDA(cudaGetLastError());
-  return RESET_OK;
+  if (t->hier)
+    return ir_run<true>(t, t->d_desc, docs, query, qoff, nq, sl_off, total_slices, res_off,
+                        res, stage, sl_cnt, pos, cnt, packed_off, st);
+  return ir_run<false>(t, t->d_desc, docs, query, qoff, nq, sl_off, total_slices, res_off,
+                       res, stage, sl_cnt, pos, cnt, packed_off, st);
 }
 
 }  // namespace rst
@@ -610,9 +699,13 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   int64_t* d_sl = nullptr;
   int64_t* d_tot = nullptr;
   int32_t* d_slc = nullptr;
+  int64_t* d_pos = nullptr;
+  int32_t* d_stage = nullptr;
   void* d_tmp = nullptr;
   reset_status rs = RESET_OK;
   auto cleanup = [&]() {
+    if (d_pos) cudaFreeAsync(d_pos, st);
+    if (d_stage) cudaFreeAsync(d_stage, st);
     if (d_sl) cudaFreeAsync(d_sl, st);
     if (d_tot) cudaFreeAsync(d_tot, st);
     if (d_slc) cudaFreeAsync(d_slc, st);
@@ -644,22 +737,17 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   IR_CUDA(cudaMemcpyAsync(&total, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   IR_CUDA(cudaStreamSynchronize(st));
   IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_slc), sizeof(int32_t) * (total > 0 ? total : 1), st));
-  if (total > 0) {
-#define IR_LAUNCH(H)                                                           \
-    do {                                                                       \
-      const int64_t g = clamp_grid((total + kWarps - 1) / kWarps,              \
-                                   persistent_grid((const void*)ir_slice_kernel<H>)); \
-      note_launch(); ir_slice_kernel<H><<<(int)g, kThreads, 0, st>>>(                         \
-          ds.desc, t->n, d_docs, d_query, d_qoff, nq, d_sl, d_res_off, d_res,  \
-          d_slc, t->d_table, t->bucket_num, t->bucket, t->lg_max, t->d_status); \
-    } while (0)
-    if (t->hier) IR_LAUNCH(true); else IR_LAUNCH(false);
-#undef IR_LAUNCH
-    IR_CUDA(cudaGetLastError());
+  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_pos), sizeof(int64_t) * (total + 1), st));
+  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_stage),
+                          sizeof(int32_t) * (size_t)(total > 0 ? total : 1) * kIrSlice, st));
+  rs = t->hier ? ir_run<true>(t, ds.desc, d_docs, d_query, d_qoff, nq, d_sl, total, d_res_off,
+                              d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st)
+               : ir_run<false>(t, ds.desc, d_docs, d_query, d_qoff, nq, d_sl, total, d_res_off,
+                               d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st);
+  if (rs != RESET_OK) {
+    cleanup();
+    return rs;
   }
-  note_launch(); ir_compact_kernel<<<(int)clamp_grid((nq + kWarps - 1) / kWarps, sm_count() * 8), kThreads, 0, st>>>(
-      d_sl, nq, d_res_off, d_res, d_slc, d_cnt);
-  IR_CUDA(cudaGetLastError());
 #undef IR_CUDA
   cleanup();
   return RESET_OK;

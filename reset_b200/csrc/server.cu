@@ -38,7 +38,8 @@ reset_status ir_launch_planned(const reset_table* t, const int32_t* docs,
                                const int32_t* query, const int32_t* qoff,
                                int32_t nq, const int64_t* sl_off,
                                int64_t total_slices, const int64_t* res_off,
-                               int32_t* res, int32_t* sl_cnt, int32_t* cnt,
+                               int32_t* res, int32_t* stage, int32_t* sl_cnt,
+                               int64_t* pos, int32_t* cnt, int64_t* packed_off,
                                cudaStream_t st);
 int ir_slice_size();
 }  // namespace rst
@@ -228,6 +229,9 @@ struct Group {
   size_t in[4] = {0, 0, 0, 0};
   size_t out[2] = {0, 0};
   size_t sc[3] = {0, 0, 0};
+  size_t sc3 = 0;
+  int64_t dense_n = 0;      // IR: survivors packed on the device
+  size_t dense_host = 0;    // IR: their offset (ints) in the slot's result buffer
 };
 
 struct Batch {
@@ -238,13 +242,16 @@ struct Batch {
   size_t in_bytes = 0, out_begin = 0, out_end = 0, d_bytes = 0;
   int64_t reserved = 0;
   int64_t t_launch = 0;
+  int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
   reset_status status = RESET_OK;
 };
 
 struct Slot {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
-  Pinned in, out;
+  Pinned in, out, res;
+  void* arena = nullptr;  // device buffer reused by this slot's batches
+  size_t arena_cap = 0;
   std::unique_ptr<Batch> batch;  // set while in flight
 };
 
@@ -267,6 +274,7 @@ struct reset_server {
   std::thread worker;
   int64_t n_done = 0, n_batches = 0, sum_batch = 0, max_batch = 0;
   int64_t max_in_use = 0, max_inflight = 0, inflight = 0;
+  int64_t launch_ns = 0, batch_ns = 0;
 };
 
 namespace {
@@ -286,7 +294,8 @@ reset_status plan_request(const reset_server* s, Req* r) {
         if (t < 0 || t >= ix.n()) return arg_fail("IR term out of range");
       const int64_t df = r->a.empty() ? 0 : ix.h_off[r->a[0] + 1] - ix.h_off[r->a[0]];
       r->aux = df;
-      r->dev_bytes = 4 * (int64_t)r->a.size() + 24 + 8 * df + 4 * ((df + slice - 1) / slice);
+      const int64_t ns = (df + slice - 1) / slice;
+      r->dev_bytes = 4 * (int64_t)r->a.size() + 32 + 4 * df + (4 * slice + 12) * ns;
       break;
     }
     case RESET_REQ_PAIRS: {
@@ -442,8 +451,8 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   for (auto& g : bt.groups) {
     switch (g.kind) {
       case RESET_REQ_IR:
-        g.out[0] = take(4 * g.items);  // counts
-        g.out[1] = take(4 * g.aux);    // results
+        g.out[0] = take(4 * g.items);        // counts
+        g.out[1] = take(8 * (g.items + 1));  // dense offsets (last = total)
         break;
       case RESET_REQ_PAIRS:
         g.out[0] = take(4 * g.items);  // intersection sizes
@@ -463,7 +472,12 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   bt.out_end = p;
   for (auto& g : bt.groups) {
     switch (g.kind) {
-      case RESET_REQ_IR: g.sc[0] = take(4 * g.aux2); break;  // slice counts
+      case RESET_REQ_IR:
+        g.sc[0] = take(4 * g.aux2);                      // slice counts
+        g.sc[1] = take(4 * (size_t)g.aux2 * slice);      // slice stage
+        g.sc[2] = take(4 * g.aux);                       // survivors, packed
+        g.sc3 = take(8 * ((size_t)g.aux2 + 1));          // slice positions
+        break;
       case RESET_REQ_TC_VERTEX:
         g.sc[0] = take(4 * g.aux);  // pa
         g.sc[1] = take(4 * g.aux);  // pb
@@ -545,7 +559,15 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
 
   // ---- device work
   cudaStream_t st = sl.st;
-  RST_CUDA(cudaMallocFromPoolAsync(&bt.d_buf, bt.d_bytes, s->pool, st));
+  if (bt.d_bytes > sl.arena_cap) {  // grow (stream-ordered; the slot is idle)
+    if (sl.arena) RST_CUDA(cudaFreeAsync(sl.arena, st));
+    sl.arena = nullptr;
+    sl.arena_cap = 0;
+    const size_t cap = std::max(bt.d_bytes, (size_t)(1u << 20));
+    RST_CUDA(cudaMallocFromPoolAsync(&sl.arena, cap, s->pool, st));
+    sl.arena_cap = cap;
+  }
+  bt.d_buf = sl.arena;
   char* dp = static_cast<char*>(bt.d_buf);
   RST_CUDA(cudaMemcpyAsync(dp, hp, bt.in_bytes, cudaMemcpyHostToDevice, st));
   for (auto& g : bt.groups) {
@@ -555,11 +577,13 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
         RST_CHECK(ir_launch_planned(
             ix.t, ix.d_elems, reinterpret_cast<int32_t*>(dp + g.in[0]),
             reinterpret_cast<int32_t*>(dp + g.in[1]), (int32_t)g.items,
-            reinterpret_cast<int64_t*>(dp + g.in[3]), g.aux2,
-            reinterpret_cast<int64_t*>(dp + g.in[2]),
-            reinterpret_cast<int32_t*>(dp + g.out[1]),
+            reinterpret_cast<int64_t*>(dp + g.in[3]), g.aux2, nullptr,
+            reinterpret_cast<int32_t*>(dp + g.sc[2]),
+            reinterpret_cast<int32_t*>(dp + g.sc[1]),
             reinterpret_cast<int32_t*>(dp + g.sc[0]),
-            reinterpret_cast<int32_t*>(dp + g.out[0]), st));
+            reinterpret_cast<int64_t*>(dp + g.sc3),
+            reinterpret_cast<int32_t*>(dp + g.out[0]),
+            reinterpret_cast<int64_t*>(dp + g.out[1]), st));
         break;
       }
       case RESET_REQ_PAIRS: {
@@ -638,7 +662,8 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
     switch (r->kind) {
       case RESET_REQ_IR: {
         const int32_t c = reinterpret_cast<const int32_t*>(at(g.out[0]))[r->item0];
-        const int32_t* res = reinterpret_cast<const int32_t*>(at(g.out[1])) + r->res0;
+        const int64_t o = reinterpret_cast<const int64_t*>(at(g.out[1]))[r->item0];
+        const int32_t* res = static_cast<const int32_t*>(sl.res.p) + g.dense_host + o;
         r->count = c;
         r->docs.assign(res, res + c);
         break;
@@ -692,6 +717,43 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
   }
 }
 
+// After the kernels: copies every IR group's packed survivors (sizes now
+// known on the host) into the slot's pinned result buffer.  Returns true if
+// copies were enqueued (the batch completes at the next event).
+bool enqueue_results(Slot& sl, Batch& bt) {
+  const char* hp = static_cast<const char*>(sl.out.p);
+  size_t total = 0;
+  for (auto& g : bt.groups) {
+    if (g.kind != RESET_REQ_IR) continue;
+    g.dense_n = reinterpret_cast<const int64_t*>(hp + (g.out[1] - bt.out_begin))[g.items];
+    g.dense_host = total;
+    total += (size_t)g.dense_n;
+  }
+  if (total == 0) return false;
+  if (sl.res.ensure(4 * total) != cudaSuccess) {
+    bt.status = cuda_fail(cudaErrorMemoryAllocation, "pinned result buffer", __FILE__, __LINE__);
+    return false;
+  }
+  const char* dp = static_cast<const char*>(bt.d_buf);
+  for (auto& g : bt.groups) {
+    if (g.kind != RESET_REQ_IR || g.dense_n == 0) continue;
+    cudaError_t e = cudaMemcpyAsync(static_cast<int32_t*>(sl.res.p) + g.dense_host,
+                                    dp + g.sc[2], 4 * (size_t)g.dense_n,
+                                    cudaMemcpyDeviceToHost, sl.st);
+    if (e != cudaSuccess) {
+      bt.status = cuda_fail(e, "result copy", __FILE__, __LINE__);
+      return false;
+    }
+  }
+  cudaError_t e = cudaEventRecord(sl.ev, sl.st);
+  if (e != cudaSuccess) {
+    bt.status = cuda_fail(e, "cudaEventRecord", __FILE__, __LINE__);
+    return false;
+  }
+  bt.phase = 1;
+  return true;
+}
+
 void worker_main(reset_server* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -705,10 +767,16 @@ void worker_main(reset_server* s) {
       std::unique_ptr<Batch> bt = std::move(sl.batch);
       lk.unlock();
       if (q != cudaSuccess) bt->status = cuda_fail(q, "server batch", __FILE__, __LINE__);
+      if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(sl, *bt)) {
+        lk.lock();
+        sl.batch = std::move(bt);  // survivors in flight
+        progressed = true;
+        continue;
+      }
       if (bt->status == RESET_OK) unpack_batch(s, sl, *bt);
-      if (bt->d_buf) cudaFreeAsync(bt->d_buf, sl.st);
       const int64_t t = now_ns();
       lk.lock();
+      s->batch_ns += t - bt->t_launch;
       for (auto& r : bt->reqs) {
         if (bt->status != RESET_OK) r->status = bt->status;
         r->t_done = t;
@@ -762,11 +830,13 @@ void worker_main(reset_server* s) {
       lk.unlock();
       bt->t_launch = t;
       reset_status rs = launch_batch(s, sl, *bt);
+      const int64_t t_launched = now_ns();
       if (rs != RESET_OK) {
         bt->status = rs;
         cudaEventRecord(sl.ev, sl.st);  // completes once the slot drains
       }
       lk.lock();
+      s->launch_ns += t_launched - t;
       sl.batch = std::move(bt);
       progressed = true;
     }
@@ -949,6 +1019,11 @@ reset_status reset_server_stats(reset_server* s, reset_server_counters* st) {
   st->budget_bytes = s->budget;
   st->in_use_bytes = s->in_use;
   st->max_in_use_bytes = s->max_in_use;
+  st->launch_host_us = s->launch_ns / 1e3;
+  st->batch_us = s->batch_ns / 1e3;
+  int64_t arena = 0;
+  for (auto& sl : s->slots) arena += (int64_t)sl.arena_cap;
+  st->arena_bytes = arena;
   return RESET_OK;
 }
 
@@ -968,8 +1043,10 @@ reset_status reset_server_destroy(reset_server* s) {
       cudaStreamDestroy(sl.st);
     }
     if (sl.ev) cudaEventDestroy(sl.ev);
+    if (sl.arena) cudaFree(sl.arena);
     sl.in.release();
     sl.out.release();
+    sl.res.release();
   }
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;

@@ -65,23 +65,54 @@ __device__ __forceinline__ uint32_t bij(const Bij& r, uint32_t x) {
   return x;
 }
 
+// Planted near-duplicates: set i > 0 is a child with probability dup_frac;
+// its parent is the nearest root (non-child) among the 256 sets before it
+// (none: it is a root itself).  A child has its parent's size and keeps
+// each of the parent's draws with probability keep_i ~ U(keep_min, 1),
+// drawing a fresh token otherwise.
+__device__ __forceinline__ bool is_child(uint64_t seed, int64_t i, double dup) {
+  return i > 0 && unif(seed, (uint64_t)i, 0xC41DC41Dull) < dup;
+}
+__device__ __forceinline__ int64_t parent_of(uint64_t seed, int64_t i, double dup) {
+  if (!is_child(seed, i, dup)) return -1;
+  for (int64_t k = i - 1; k >= 0 && k >= i - 256; --k)
+    if (!is_child(seed, k, dup)) return k;
+  return -1;
+}
+
+__device__ __forceinline__ int root_size(uint64_t seed, int64_t i,
+                                         const double* __restrict__ cdf, int ncdf,
+                                         int lo) {
+  const double u = unif(seed, (uint64_t)i, 0xFFFFFFull);
+  int a = 0, b = ncdf - 1;  // first index with cdf >= u
+  while (a < b) {
+    int mid = (a + b) >> 1;
+    if (cdf[mid] >= u) b = mid; else a = mid + 1;
+  }
+  return lo + a;
+}
+
 __global__ void set_sizes_kernel(int32_t n, uint64_t seed,
                                  const double* __restrict__ cdf, int ncdf,
-                                 int lo, int64_t* __restrict__ sizes) {
+                                 int lo, double dup, int64_t* __restrict__ sizes) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double u = unif(seed, (uint64_t)i, 0xFFFFFFull);
-    int a = 0, b = ncdf - 1;  // first index with cdf >= u
-    while (a < b) {
-      int mid = (a + b) >> 1;
-      if (cdf[mid] >= u) b = mid; else a = mid + 1;
-    }
-    sizes[i] = lo + a;
+    const int64_t p = parent_of(seed, i, dup);
+    sizes[i] = root_size(seed, p >= 0 ? p : i, cdf, ncdf, lo);
   }
+}
+
+__device__ __forceinline__ uint32_t draw_token(uint64_t seed, int64_t set, int64_t j,
+                                               double lnU1, uint64_t U, const Bij& bj) {
+  const double u = unif(seed, (uint64_t)set, (uint64_t)j + 1);
+  uint64_t rank = (uint64_t)floor(exp(u * lnU1)) - 1;
+  if (rank >= U) rank = U - 1;
+  return bij(bj, (uint32_t)rank);
 }
 
 // One warp per set: its draws as (set << ulog) | token keys.
 __global__ void draw_tokens_kernel(int32_t n, uint64_t seed, int ulog, Bij bj,
+                                   double dup, double keep_min,
                                    const int64_t* __restrict__ draw_off,
                                    uint64_t* __restrict__ keys) {
   const int lane = threadIdx.x & 31;
@@ -90,11 +121,14 @@ __global__ void draw_tokens_kernel(int32_t n, uint64_t seed, int ulog, Bij bj,
   for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n;
        i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
     const int64_t b0 = draw_off[i], b1 = draw_off[i + 1];
+    const int64_t p = parent_of(seed, i, dup);
+    const double keep = keep_min + (1.0 - keep_min) * unif(seed, (uint64_t)i, 0xEEEEull);
     for (int64_t j = b0 + lane; j < b1; j += 32) {
-      const double u = unif(seed, (uint64_t)i, (uint64_t)(j - b0) + 1);
-      uint64_t rank = (uint64_t)floor(exp(u * lnU1)) - 1;
-      if (rank >= U) rank = U - 1;
-      const uint32_t tok = bij(bj, (uint32_t)rank);
+      uint32_t tok;
+      if (p >= 0 && unif(seed ^ 0x6B6565700000ull, (uint64_t)i, (uint64_t)(j - b0)) < keep)
+        tok = draw_token(seed, p, j - b0, lnU1, U, bj);
+      else
+        tok = draw_token(seed, i, j - b0, lnU1, U, bj);
       keys[j] = ((uint64_t)i << ulog) | tok;
     }
   }
@@ -265,7 +299,8 @@ using namespace rst;
 
 extern "C" reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2,
                                              double size_s, int32_t size_lo,
-                                             int32_t size_hi, uint64_t seed,
+                                             int32_t size_hi, double dup_frac,
+                                             double keep_min, uint64_t seed,
                                              int32_t** d_off_out,
                                              int32_t** d_tokens_out,
                                              int64_t* m_out,
@@ -274,6 +309,8 @@ extern "C" reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2,
   if (n < 1 || n >= (1 << 21)) return arg_fail("n must be in 1..2^21-1");
   if (universe_log2 < 4 || universe_log2 > 24) return arg_fail("universe_log2 in 4..24");
   if (size_lo < 1 || size_hi < size_lo || size_hi > 16384) return arg_fail("size range");
+  if (!(dup_frac >= 0.0 && dup_frac < 1.0)) return arg_fail("dup_frac must be in [0, 1)");
+  if (!(keep_min >= 0.0 && keep_min <= 1.0)) return arg_fail("keep_min must be in [0, 1]");
   cudaStream_t st = as_stream(stream);
   const int ncdf = size_hi - size_lo + 1;
   std::vector<double> cdf(ncdf);
@@ -292,7 +329,8 @@ extern "C" reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2,
   RST_CUDA(tmp.get(&d_doff, sizeof(int64_t) * (n + 1)));
   RST_CUDA(cudaMemcpyAsync(d_cdf, cdf.data(), sizeof(double) * ncdf, cudaMemcpyHostToDevice, st));
   note_launch();
-  set_sizes_kernel<<<g_grid(n), 256, 0, st>>>(n, seed, d_cdf, ncdf, size_lo, d_sizes);
+  set_sizes_kernel<<<g_grid(n), 256, 0, st>>>(n, seed, d_cdf, ncdf, size_lo, dup_frac,
+                                               d_sizes);
   RST_CUDA(cudaGetLastError());
   RST_CUDA(cudaMemsetAsync(d_sizes + n, 0, sizeof(int64_t), st));
   size_t tb = 0;
@@ -308,7 +346,7 @@ extern "C" reset_status reset_gen_token_sets(int32_t n, int32_t universe_log2,
   RST_CUDA(tmp.get(&k1, sizeof(uint64_t) * nd));
   note_launch();
   draw_tokens_kernel<<<g_grid((int64_t)n * 32), 256, 0, st>>>(
-      n, seed, universe_log2, make_bij(seed, universe_log2), d_doff, k0);
+      n, seed, universe_log2, make_bij(seed, universe_log2), dup_frac, keep_min, d_doff, k0);
   RST_CUDA(cudaGetLastError());
   const int endbit = universe_log2 + 21;
   cub::DoubleBuffer<uint64_t> db(k0, k1);

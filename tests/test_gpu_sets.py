@@ -42,6 +42,17 @@ def test_token_sets_properties(R, n, ulog, lo, hi):
     assert np.array_equal(host(off2), o) and np.array_equal(host(tok2), t)
 
 
+def test_planted_near_duplicates(R):
+    off, tok = R.gen_token_sets(3000, 24, 1.2, 8, 200, seed=0x5EED0D0D, dup_frac=0.4, keep_min=0.9)
+    o, t = host(off), host(tok)
+    rows = [set(t[o[i]:o[i + 1]].tolist()) for i in range(o.size - 1)]
+    close = sum(1 for i in range(1, len(rows)) if any(
+        len(rows[i] & rows[k]) >= 0.7 * len(rows[i] | rows[k]) for k in range(max(0, i - 8), i)))
+    assert close > 0.2 * len(rows)       # a large share of sets has a near twin
+    off0, tok0 = R.gen_token_sets(3000, 24, 1.2, 8, 200, seed=0x5EED0D0D)
+    assert not np.array_equal(host(tok0), t)
+
+
 def test_token_sets_rejects_bad_arguments(R):
     from reset_b200._lib import ResetError
     for args in [(0, 10, 1.5, 1, 4), (1 << 21, 10, 1.5, 1, 4), (10, 3, 1.5, 1, 4),
@@ -50,11 +61,11 @@ def test_token_sets_rejects_bad_arguments(R):
             R.gen_token_sets(*args)
 
 
-@pytest.mark.parametrize("n,ulog,lo,hi,num,den", [
-    (400, 7, 2, 30, 1, 2), (1500, 9, 4, 40, 7, 10), (1200, 8, 1, 12, 3, 4),
-    (900, 10, 10, 60, 9, 10), (60, 4, 1, 16, 1, 1)])
-def test_prefix_candidates_match_oracle(R, oracle_mod, n, ulog, lo, hi, num, den):
-    off, tok = R.gen_token_sets(n, ulog, 1.3, lo, hi, seed=0x5EED1000 + n)
+@pytest.mark.parametrize("n,ulog,lo,hi,num,den,dup", [
+    (400, 7, 2, 30, 1, 2, 0.0), (1500, 9, 4, 40, 7, 10, 0.0), (1200, 8, 1, 12, 3, 4, 0.0),
+    (900, 10, 10, 60, 9, 10, 0.0), (60, 4, 1, 16, 1, 1, 0.0), (1500, 20, 8, 80, 7, 10, 0.3)])
+def test_prefix_candidates_match_oracle(R, oracle_mod, n, ulog, lo, hi, num, den, dup):
+    off, tok = R.gen_token_sets(n, ulog, 1.3, lo, hi, seed=0x5EED1000 + n, dup_frac=dup)
     pa, pb = R.prefix_candidates(off, tok, ulog, num, den)
     a, b = host(pa), host(pb)
     assert np.all(a < b)
@@ -66,11 +77,11 @@ def test_prefix_candidates_match_oracle(R, oracle_mod, n, ulog, lo, hi, num, den
     assert _pairs(ja, jb) <= _pairs(a, b)        # no qualifying pair is lost
 
 
-@pytest.mark.parametrize("hier", [True, False])
-def test_self_join_pipeline_equals_brute_force(R, oracle_mod, cuda, hier):
+@pytest.mark.parametrize("hier,ulog,dup", [(True, 9, 0.0), (False, 9, 0.0), (True, 22, 0.3)])
+def test_self_join_pipeline_equals_brute_force(R, oracle_mod, cuda, hier, ulog, dup):
     torch = cuda
-    n, ulog, num, den = 1500, 9, 7, 10
-    off, tok = R.gen_token_sets(n, ulog, 1.3, 4, 40, seed=0x5EED2000)
+    n, num, den = 1500, 7, 10
+    off, tok = R.gen_token_sets(n, ulog, 1.3, 4, 40, seed=0x5EED2000, dup_frac=dup)
     t = R.Table(off, tok, hierarchical=hier)
     pa, pb = R.prefix_candidates(off, tok, ulog, num, den)
     batch = R.Batch(t, tok, capacity=max(1, pa.numel()), num=num, den=den)
