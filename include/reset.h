@@ -134,9 +134,10 @@ reset_status reset_tc_count(const reset_table *t, const int32_t *d_off,
 
 /* reset_tc_count with an explicit method (same count either way):
  *   0 = default (1, the faster on B200 as measured);
- *   1 = edge-flattened: 32 edges per warp; pairs of >= 32 keys probed by the
- *       whole warp, smaller ones flattened across the lanes, both sides read
- *       from HBM (the reference's access pattern);
+ *   1 = edge-flattened: 32 edges per warp; pairs with at least
+ *       warp_pair_min keys (reset_tuning, default 64) probed by the whole
+ *       warp, smaller ones flattened across the lanes, both sides read from
+ *       HBM (the reference's access pattern);
  *   2 = vertex-staged: each row staged once in shared memory (keys + hash
  *       set) and reused by all its out-edges. */
 reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
