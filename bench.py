@@ -58,8 +58,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--probe-rounds", type=int, default=0, choices=[0, 2, 4])
+    ap.add_argument("--probe-rounds", type=int, default=0, choices=[0, 2, 4, 8])
     ap.add_argument("--warp-pair-min", type=int, default=0)
+    ap.add_argument("--probe-variant", type=int, default=-1, choices=[-1, 0, 1],
+                    help="-1 library default; 0 pipelined; 1 lean whole-warp pair loop")
     ap.add_argument("--tc-method", type=int, default=0, choices=[0, 1, 2],
                     help="0 default (edge-flattened), 1 edge-flattened, 2 vertex-staged")
     ap.add_argument("--workload", default="tc",
@@ -195,9 +197,10 @@ def run_ours(a, rank, world, local):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     L = _lib.load()
-    if a.probe_rounds or a.warp_pair_min:
+    if a.probe_rounds or a.warp_pair_min or a.probe_variant >= 0:
         api.set_tuning(probe_rounds=a.probe_rounds or None,
-                       warp_pair_min=a.warp_pair_min or None)
+                       warp_pair_min=a.warp_pair_min or None,
+                       probe_variant=a.probe_variant if a.probe_variant >= 0 else None)
 
     off, cols = api.gen_rmat(a.scale, a.edge_factor, SEED)
     n, m = off.numel() - 1, cols.numel()

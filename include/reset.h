@@ -393,9 +393,12 @@ reset_status reset_server_destroy(reset_server *s);
 /* Process-wide kernel knobs (no counterpart in the reference, whose launch
  * shapes are compile-time constants).  Results never depend on them. */
 typedef struct reset_tuning {
-  int32_t probe_rounds;  /* 2 or 4: probe rounds a warp keeps in flight     */
+  int32_t probe_rounds;  /* 2, 4 (or 8 with variant 1): probe rounds a warp
+                            keeps in flight                                 */
   int32_t warp_pair_min; /* pairs with >= this many keys get a whole warp   */
-  int32_t reserved[6];
+  int32_t probe_variant; /* whole-warp pair loop: 0 = software-pipelined,
+                            1 = lean (branch-free resolve, no prefetch)     */
+  int32_t reserved[5];
 } reset_tuning;
 
 reset_status reset_get_tuning(reset_tuning *out);

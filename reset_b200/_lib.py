@@ -32,7 +32,7 @@ class Params(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("probe_rounds", C.c_int32), ("warp_pair_min", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("probe_variant", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class TableView(C.Structure):

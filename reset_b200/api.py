@@ -233,16 +233,20 @@ def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 0x5EED0016,
 def get_tuning() -> dict:
     t = Tuning()
     check(_lib().reset_get_tuning(C.byref(t)))
-    return {"probe_rounds": t.probe_rounds, "warp_pair_min": t.warp_pair_min}
+    return {"probe_rounds": t.probe_rounds, "warp_pair_min": t.warp_pair_min,
+            "probe_variant": t.probe_variant}
 
 
-def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] = None):
+def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] = None,
+               probe_variant: Optional[int] = None):
     t = Tuning()
     check(_lib().reset_get_tuning(C.byref(t)))
     if probe_rounds is not None:
         t.probe_rounds = probe_rounds
     if warp_pair_min is not None:
         t.warp_pair_min = warp_pair_min
+    if probe_variant is not None:
+        t.probe_variant = probe_variant
     check(_lib().reset_set_tuning(C.byref(t)))
 
 

@@ -12,7 +12,7 @@ namespace rst {
 static thread_local char g_err[512] = "";
 static std::atomic<long long> g_launches{0};
 static std::mutex g_tune_mu;
-static reset_tuning g_tune = {4, 64, {0, 0, 0, 0, 0, 0}};
+static reset_tuning g_tune = {8, 64, 1, {0, 0, 0, 0, 0}};
 
 reset_tuning tuning() {
   std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -94,10 +94,14 @@ reset_status reset_get_tuning(reset_tuning* out) {
 
 reset_status reset_set_tuning(const reset_tuning* in) {
   if (!in) return rst::arg_fail("NULL tuning");
-  if (in->probe_rounds != 2 && in->probe_rounds != 4)
-    return rst::arg_fail("probe_rounds must be 2 or 4");
+  if (in->probe_rounds != 2 && in->probe_rounds != 4 && in->probe_rounds != 8)
+    return rst::arg_fail("probe_rounds must be 2, 4 or 8");
+  if (in->probe_rounds == 8 && in->probe_variant != 1)
+    return rst::arg_fail("probe_rounds 8 needs probe_variant 1");
   if (in->warp_pair_min < 1 || in->warp_pair_min > (1 << 20))
     return rst::arg_fail("warp_pair_min must be in 1..2^20");
+  if (in->probe_variant != 0 && in->probe_variant != 1)
+    return rst::arg_fail("probe_variant must be 0 or 1");
   std::lock_guard<std::mutex> lock(rst::g_tune_mu);
   rst::g_tune = *in;
   return RESET_OK;

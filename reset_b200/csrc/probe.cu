@@ -55,8 +55,8 @@ __device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
 
 // ----------------------------------------------------------------- TC ----
 
-template <bool HIER, int ROUNDS>
-__global__ void __launch_bounds__(kThreads)
+template <bool HIER, int ROUNDS, bool LEAN>
+__global__ void __launch_bounds__(kThreads, 4)
     tc_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ off,
               const int32_t* __restrict__ cols,
               const int32_t* __restrict__ chunk_row, int32_t n, int64_t m,
@@ -109,8 +109,12 @@ __global__ void __launch_bounds__(kThreads)
       const int ka = __shfl_sync(kFull, A.x, k);
       const int klg = __shfl_sync(kFull, blg, k);
       const int64_t kt = __shfl_sync(kFull, bt, k);
-      hits += warp_probe_pair<HIER, ROUNDS>(cols + ka, ks, table + kt, klg, lg_max,
-                                            bn, b, status, s_qx[warp], s_qh[warp]);
+      if (LEAN)
+        hits += warp_probe_pair_lean<HIER, ROUNDS>(cols + ka, ks, table + kt, klg, lg_max,
+                                                   bn, b, status, s_qx[warp], s_qh[warp]);
+      else
+        hits += warp_probe_pair<HIER, ROUNDS>(cols + ka, ks, table + kt, klg, lg_max,
+                                              bn, b, status, s_qx[warp], s_qh[warp]);
     }
     hits += flat_probe<HIER>(cols, me, table, big ? 0 : s, A.x, bt, blg, lg_max,
                              bn, b, status, [](int) {});
@@ -121,8 +125,8 @@ __global__ void __launch_bounds__(kThreads)
 
 // ---------------------------------------------------------------- SSS ----
 
-template <bool HIER, bool FLOAT_RULE>
-__global__ void __launch_bounds__(kThreads)
+template <bool HIER, bool FLOAT_RULE, int ROUNDS, bool LEAN>
+__global__ void __launch_bounds__(kThreads, 4)
     sss_kernel(const int4* __restrict__ desc, int32_t n,
                const int32_t* __restrict__ elems, int64_t n_elems,
                const int32_t* __restrict__ pa, const int32_t* __restrict__ pb,
@@ -133,7 +137,7 @@ __global__ void __launch_bounds__(kThreads)
                uint8_t* __restrict__ flags, int32_t* __restrict__ inter,
                int32_t* __restrict__ status) {
   __shared__ int s_hits[kWarps][32];
-  __shared__ int s_qx[kWarps][32 * 4], s_qh[kWarps][32 * 4];
+  __shared__ int s_qx[kWarps][32 * ROUNDS], s_qh[kWarps][32 * ROUNDS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (np_dev) np = *np_dev;  // pair count set on the device (captured graphs)
   const int64_t n_chunks = (np + 31) >> 5;
@@ -179,8 +183,11 @@ __global__ void __launch_bounds__(kThreads)
       const int ka = __shfl_sync(kFull, A.x, k);
       const int klg = __shfl_sync(kFull, blg, k);
       const int64_t kt = __shfl_sync(kFull, bt, k);
-      int h = warp_probe_pair<HIER, 4>(elems + ka, ks, table + kt, klg, lg_max, bn,
-                                       b, status, s_qx[warp], s_qh[warp]);
+      int h = LEAN ? warp_probe_pair_lean<HIER, ROUNDS>(elems + ka, ks, table + kt, klg,
+                                                        lg_max, bn, b, status, s_qx[warp],
+                                                        s_qh[warp])
+                   : warp_probe_pair<HIER, ROUNDS>(elems + ka, ks, table + kt, klg, lg_max,
+                                                   bn, b, status, s_qx[warp], s_qh[warp]);
       h = __reduce_add_sync(kFull, h);
       if (lane == 0) s_hits[warp][k] += h;
       __syncwarp();
@@ -496,18 +503,23 @@ reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
                                    unsigned long long* cursor, int64_t capacity,
                                    int32_t num, int32_t den, uint8_t* flags,
                                    int32_t* inter, cudaStream_t st) {
-  const int wpm = tuning().warp_pair_min;
-#define SSS_P(H)                                                               \
+  const reset_tuning tun = tuning();
+  const int wpm = tun.warp_pair_min;
+#define SSS_P(H, R, LN)                                                        \
   do {                                                                         \
     const int64_t g = clamp_grid(((capacity + 31) / 32 + kWarps - 1) / kWarps, \
-                                 persistent_grid((const void*)sss_kernel<H, false>)); \
+                                 persistent_grid((const void*)sss_kernel<H, false, R, LN>)); \
     note_launch();                                                             \
-    sss_kernel<H, false><<<(int)g, kThreads, 0, st>>>(                         \
+    sss_kernel<H, false, R, LN><<<(int)g, kThreads, 0, st>>>(                  \
         t->d_desc, t->n, elems, t->m, pa, pb, capacity, np_dev, cursor,        \
         t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, 0.f, wpm,   \
         flags, inter, t->d_status);                                            \
   } while (0)
-  if (t->hier) SSS_P(true); else SSS_P(false);
+  if (tun.probe_variant == 1) {
+    if (t->hier) SSS_P(true, 8, true); else SSS_P(false, 8, true);
+  } else {
+    if (t->hier) SSS_P(true, 4, false); else SSS_P(false, 4, false);
+  }
 #undef SSS_P
   RST_CUDA(cudaGetLastError());
   return RESET_OK;
@@ -568,20 +580,33 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(*cursor), st);
   const reset_tuning tun = tuning();
   const int wpm = tun.warp_pair_min;
-#define TC_LAUNCH(H, R)                                                        \
+#define TC_LAUNCH(H, R, LN)                                                    \
   do {                                                                         \
     const int64_t g = clamp_grid(((m + 31) / 32 + kWarps - 1) / kWarps,        \
-                                 persistent_grid((const void*)tc_kernel<H, R>)); \
+                                 persistent_grid((const void*)tc_kernel<H, R, LN>)); \
     note_launch();                                                             \
-    tc_kernel<H, R><<<(int)g, kThreads, 0, st>>>(                              \
+    tc_kernel<H, R, LN><<<(int)g, kThreads, 0, st>>>(                          \
         ds.desc, d_off, d_cols, rows, t->n, m, t->d_table, t->bucket_num,      \
         t->bucket, t->lg_max, cnt, cursor, wpm, t->d_status);                  \
   } while (0)
   if (e == cudaSuccess) {
+    const bool lean = tun.probe_variant == 1;
     if (t->hier) {
-      if (tun.probe_rounds == 2) TC_LAUNCH(true, 2); else TC_LAUNCH(true, 4);
+      if (lean) {
+        if (tun.probe_rounds == 2) TC_LAUNCH(true, 2, true);
+        else if (tun.probe_rounds == 8) TC_LAUNCH(true, 8, true);
+        else TC_LAUNCH(true, 4, true);
+      } else {
+        if (tun.probe_rounds == 2) TC_LAUNCH(true, 2, false); else TC_LAUNCH(true, 4, false);
+      }
     } else {
-      if (tun.probe_rounds == 2) TC_LAUNCH(false, 2); else TC_LAUNCH(false, 4);
+      if (lean) {
+        if (tun.probe_rounds == 2) TC_LAUNCH(false, 2, true);
+        else if (tun.probe_rounds == 8) TC_LAUNCH(false, 8, true);
+        else TC_LAUNCH(false, 4, true);
+      } else {
+        if (tun.probe_rounds == 2) TC_LAUNCH(false, 2, false); else TC_LAUNCH(false, 4, false);
+      }
     }
     e = cudaGetLastError();
   }
@@ -612,20 +637,27 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   cudaStream_t st = as_stream(stream);
   DescScope ds;
   RST_CHECK(resolve_desc(t, d_off, st, &ds));
-#define SSS_LAUNCH(H, F)                                                     \
+  const reset_tuning tun = tuning();
+#define SSS_LAUNCH(H, F, R, LN)                                              \
   do {                                                                       \
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
-                                 persistent_grid((const void*)sss_kernel<H, F>)); \
-    note_launch(); sss_kernel<H, F><<<(int)g, kThreads, 0, st>>>(             \
+                                 persistent_grid((const void*)sss_kernel<H, F, R, LN>)); \
+    note_launch(); sss_kernel<H, F, R, LN><<<(int)g, kThreads, 0, st>>>(      \
         ds.desc, t->n, d_elems, t->m, d_pa, d_pb, np, nullptr, nullptr,      \
         t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, thr,       \
-        tuning().warp_pair_min, d_flags, d_inter, t->d_status);               \
+        tun.warp_pair_min, d_flags, d_inter, t->d_status);                    \
+  } while (0)
+#define SSS_V(H, F)                                                          \
+  do {                                                                       \
+    if (tun.probe_variant == 1) SSS_LAUNCH(H, F, 8, true);                   \
+    else SSS_LAUNCH(H, F, 4, false);                                         \
   } while (0)
   if (t->hier) {
-    if (float_rule) SSS_LAUNCH(true, true); else SSS_LAUNCH(true, false);
+    if (float_rule) SSS_V(true, true); else SSS_V(true, false);
   } else {
-    if (float_rule) SSS_LAUNCH(false, true); else SSS_LAUNCH(false, false);
+    if (float_rule) SSS_V(false, true); else SSS_V(false, false);
   }
+#undef SSS_V
 #undef SSS_LAUNCH
   RST_CUDA(cudaGetLastError());
   return RESET_OK;

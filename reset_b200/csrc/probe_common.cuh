@@ -42,18 +42,52 @@ __device__ __forceinline__ bool probe_rest(int x, const int32_t* __restrict__ tb
     k = 0;
     h = (h + 1) & (l - 1);
   }
+  // walk with a running slot pointer (one multiply up front)
+  const int32_t* __restrict__ p = tb + h + (int64_t)k * bn;
   const int64_t cap = (int64_t)l * b;
   for (int64_t t = 1; t < cap; ++t) {
-    const int s = __ldg(tb + h + (int64_t)k * bn);
+    const int s = __ldg(p);
     if (s == x) return true;
     if (s == -1) return false;
     if (++k == b) {
       k = 0;
       h = (h + 1) & (l - 1);
+      p = tb + h;
+    } else {
+      p += bn;
     }
   }
   atomicOr(status, kErrProbeLimit);
   return false;
+}
+
+// Queue walk: continues a probe from slot k of bucket h with a running slot
+// pointer and a 32-bit step count; walks longer than 64 slots (a crowded
+// region) finish in probe_rest.  Same answer as probe_rest.
+template <bool HIER>
+__device__ __forceinline__ bool probe_walk(int x, const int32_t* __restrict__ tb,
+                                           int lg, int h, int k, int64_t bn, int b,
+                                           int32_t* status) {
+  const int lmask = (1 << lg) - 1;
+  if (k == b) {
+    k = 0;
+    h = (h + 1) & lmask;
+  }
+  const int32_t* __restrict__ p = tb + h + (int64_t)k * bn;
+#pragma unroll 1
+  for (int t = 0; t < 64; ++t) {
+    const int s = __ldg(p);
+    if (s == x) return true;
+    if (s == -1) return false;
+    if (++k == b) {
+      k = 0;
+      h = (h + 1) & lmask;
+      p = tb + h;
+    } else {
+      p += bn;
+    }
+  }
+  return probe_rest<HIER>(x, tb, lg, h, k, bn, b, status);
 }
 
 // Warp-inclusive scan; returns the exclusive prefix and sets *total.
@@ -180,6 +214,71 @@ __device__ __forceinline__ int warp_probe_pair(const int32_t* __restrict__ keys,
       const int k0 = b == 1 ? 1 : 2;
       for (int i = lane; i < nq; i += 32)
         hits += probe_rest<HIER>(qx[i], tb, lg, qh[i], k0, bn, b, status);
+      __syncwarp();
+    }
+  }
+  return hits;
+}
+
+// Lean whole-warp pair loop: R rounds of 32 keys per batch; per round a key
+// load, the home bucket, loads of slots 0 and 1 (independent), and a
+// branch-free resolve; probes that both slots leave open go to the warp's
+// shared-memory queue (qx/qh, 32*R entries), walked together after the
+// batch.  No prefetch across batches: latency is hidden by the other
+// resident warps.  Returns this lane's hits.
+template <bool HIER, int R>
+__device__ __forceinline__ int warp_probe_pair_lean(const int32_t* __restrict__ keys,
+                                                    int s,
+                                                    const int32_t* __restrict__ tb,
+                                                    int lg, int lg_max, int64_t bn,
+                                                    int b, int32_t* status,
+                                                    int* qx, int* qh) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const int32_t* __restrict__ tb1 = tb + (b > 1 ? bn : 0);
+  const unsigned hmask = HIER ? ((1u << lg_max) - 1u) : ((1u << lg) - 1u);
+  const int hsh = HIER ? (lg_max - lg) : 0;
+  const int k0 = b == 1 ? 1 : 2;  // where queued probes continue
+  int hits = 0;
+  for (int base = 0; base < s; base += 32 * R) {
+    const int nr = min(R, (s - base + 31) >> 5);  // rounds with keys (warp-uniform)
+    int x[R], h[R], s0[R], s1[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = base + r * 32 + lane;
+      x[r] = -2;
+      if (r < nr && j < s) x[r] = __ldg(keys + j);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      h[r] = (int)(((unsigned)x[r] & hmask) >> hsh);
+      s0[r] = -1;
+      s1[r] = -1;
+      if (r < nr && x[r] >= 0) {
+        s0[r] = __ldg(tb + h[r]);
+        s1[r] = __ldg(tb1 + h[r]);
+      }
+    }
+    int nq = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (r >= nr) break;
+      const bool e0 = s0[r] == -1, m0 = s0[r] == x[r];
+      const bool e1 = s1[r] == -1, m1 = s1[r] == x[r];
+      hits += (int)(m0 | (!e0 & m1));
+      const bool pend = (x[r] >= 0) & !m0 & !e0 & !m1 & !e1;
+      const unsigned pm = __ballot_sync(kFull, pend);
+      if (pend) {
+        const int pos = nq + __popc(pm & lt);
+        qx[pos] = x[r];
+        qh[pos] = h[r];
+      }
+      nq += __popc(pm);
+    }
+    if (nq) {
+      __syncwarp();
+      for (int i = lane; i < nq; i += 32)
+        hits += probe_walk<HIER>(qx[i], tb, lg, qh[i], k0, bn, b, status);
       __syncwarp();
     }
   }

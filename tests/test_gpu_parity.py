@@ -313,3 +313,37 @@ def test_tc_methods_agree_rmat(R, cuda, oracle_mod, scale):
     t = R.Table(off, cols, hash_order=True)
     for method in (R.TC_EDGE, R.TC_STAGED):
         assert R.tc_count(t, off, t.hash_order, method=method) == want
+
+
+# --------------------------------------------------------- tuning knobs --
+
+@pytest.mark.parametrize("variant,rounds,wpm", [(0, 2, 64), (0, 4, 1), (1, 2, 32), (1, 4, 64),
+                                                (1, 8, 64), (1, 8, 1), (1, 8, 100000)])
+def test_every_probe_variant_counts_the_same(R, cuda, oracle_mod, variant, rounds, wpm):
+    """The probe knobs change scheduling only: TC counts, SSS flags and sizes
+    equal the oracle for every variant, both hashes."""
+    torch = cuda
+    before = R.get_tuning()
+    try:
+        R.set_tuning(probe_rounds=4 if rounds != 8 else None, warp_pair_min=wpm,
+                     probe_variant=variant)
+        R.set_tuning(probe_rounds=rounds)
+        off, cols = R.gen_rmat(13, 16, 0x5EED7000, oriented=True)
+        want = oracle_mod.tc_merge(host(off), host(cols))
+        for hier in (True, False):
+            t = R.Table(off, cols, hierarchical=hier, hash_order=True)
+            assert R.tc_count(t, off, t.hash_order) == want
+            assert R.tc_count(t, off, cols) == want
+        s_off, s_cols = R.gen_rmat(11, 16, 0x5EED7001, oriented=False)
+        st = R.Table(s_off, s_cols, hierarchical=True)
+        n = s_off.numel() - 1
+        g = torch.Generator(device="cuda").manual_seed(3)
+        pa = torch.randint(0, n, (20000,), device="cuda", dtype=torch.int32, generator=g)
+        pb = torch.randint(0, n, (20000,), device="cuda", dtype=torch.int32, generator=g)
+        f, i = R.sss(st, s_off, s_cols, pa, pb, num=1, den=5)
+        of, oi = oracle_mod.sss(oracle_mod.Table(host(s_off), host(s_cols), hier=1),
+                                host(pa), host(pb), mode=1, num=1, den=5)
+        assert np.array_equal(host(f), of.astype(np.uint8)) and np.array_equal(host(i), oi)
+    finally:
+        R.set_tuning(probe_rounds=4, probe_variant=before["probe_variant"])
+        R.set_tuning(**before)
