@@ -98,6 +98,25 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+# ------------------------------------------------------- rank aggregation --
+
+def max_over_ranks(vals, world, device="cuda"):
+    """Element-wise max of per-rank timings (every rank calls it in the same
+    order; identity for one rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(vals), dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def weak_value(units_per_rank, world, ms):
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank units, timed as the slowest rank's `ms`."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 # ----------------------------------------------------------- clock sampler --
 
 class Clocks:
@@ -278,13 +297,9 @@ def run_ours(a, rank, world, local):
         del d_off, d_cols
     e2e_step = sum(e2e_ms) / len(e2e_ms)
 
-    # max over ranks
-    mx = torch.tensor([ms, e2e_step, probe_avg], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-    ms, e2e_step, probe_avg = mx.tolist()
+    ms, e2e_step, probe_avg = max_over_ranks([ms, e2e_step, probe_avg], world)
     step_ms = ms / a.steps
-    value = world * m / (step_ms / 1e3)
+    value = weak_value(m, world, step_ms)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -316,10 +331,10 @@ def run_ours(a, rank, world, local):
                    "vertex_ids": "relabeled by a seeded bijection (Graph500 convention)",
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (tables+rows > 6 GB); no flush"},
-        "e2e": {"value": world * m / (e2e_step / 1e3), "unit": UNIT,
+        "e2e": {"value": weak_value(m, world, e2e_step), "unit": UNIT,
                 "h2d_bytes_per_step": 4 * (n + 1) + 4 * m, "d2h_bytes_per_step": 8,
                 "ms_per_step": e2e_step},
-        "probe_only": {"value": world * m / (probe_avg / 1e3), "unit": UNIT,
+        "probe_only": {"value": weak_value(m, world, probe_avg), "unit": UNIT,
                        "ms_per_launch": probe_avg},
         "roofline": {"bound": "hbm",
                      "kernel": "tc_staged_kernel" if a.tc_method == 2 else "tc_kernel",
