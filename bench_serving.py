@@ -96,7 +96,7 @@ def sss_join_ours(a, rank, world, local):
     def measure(hp):
         api.set_tuning(probe_rounds=hp.probe_rounds, warp_pair_min=hp.warp_pair_min)
         t = api.Table(off, tok, alpha=hp.alpha, bucket=hp.b)
-        bt = api.Batch(t, tok, capacity=max(1, samp), num=num, den=den)
+        bt = api.Batch(t, tok, capacity=max(1, samp), num=num, den=den, decisions_only=True)
         bt.pair_a[:samp].copy_(sa)
         bt.pair_b[:samp].copy_(sb)
         ms = autotune.timed(lambda: bt.run(samp), reps=3)
@@ -105,13 +105,14 @@ def sss_join_ours(a, rank, world, local):
         return ms
 
     hp = autotune.solve("sss", sizes.cpu().numpy(), measure=measure, measure_top=3,
-                        cache=None) if samp else autotune.HyperParams()
+                        rounds=(8,), cache=None) if samp else autotune.HyperParams()
     api.set_tuning(probe_rounds=hp.probe_rounds, warp_pair_min=hp.warp_pair_min)
     del sa, sb
 
     t = api.Table(off, tok, alpha=hp.alpha, bucket=hp.b)      # resident index
     cap = max(1, P)
-    bt = api.Batch(t, tok, capacity=cap, num=num, den=den)
+    # the join needs decisions only: pairs stop as soon as they are settled
+    bt = api.Batch(t, tok, capacity=cap, num=num, den=den, decisions_only=True)
     stream = torch.cuda.current_stream()
     results = []
     rep_ev = []
@@ -152,6 +153,23 @@ def sss_join_ours(a, rank, world, local):
     for ra, _ in results:
         assert ra.numel() == want
     rep = statistics.mean(e0.elapsed_time(e1) for e0, e1 in rep_ev)
+    # the same candidates decided with full intersection sizes (every key
+    # probed): the launch the roofline's algorithmic bytes describe
+    bfull = api.Batch(t, tok, capacity=cap, num=num, den=den)
+    bfull.pair_a[:P].copy_(pa)
+    bfull.pair_b[:P].copy_(pb)
+    full_ms = []
+    for i in range(2 + a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bfull.run(P)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            full_ms.append(e0.elapsed_time(e1))
+    assert torch.equal(bfull.flags[:P], bt.flags[:P])   # same decisions
+    full = statistics.mean(full_ms)
+    bfull.close()
 
     # e2e: pinned host token sets -> index + candidates + decisions -> host pair list
     h_off, h_tok = off.cpu().pin_memory(), tok.cpu().pin_memory()
@@ -164,7 +182,8 @@ def sss_join_ours(a, rank, world, local):
         d_tok = h_tok.to("cuda", non_blocking=True)
         tt = api.Table(d_off, d_tok, alpha=hp.alpha, bucket=hp.b)
         ca, cb = api.prefix_candidates(d_off, d_tok, ulog, num, den)
-        b2 = api.Batch(tt, d_tok, capacity=max(1, ca.numel()), num=num, den=den)
+        b2 = api.Batch(tt, d_tok, capacity=max(1, ca.numel()), num=num, den=den,
+                       decisions_only=True)
         f, _ = b2(ca, cb)
         keep = f.nonzero().squeeze(1)
         pairs = torch.stack([ca[keep], cb[keep]], 1).cpu()
@@ -193,9 +212,9 @@ def sss_join_ours(a, rank, world, local):
     plain_s = time.perf_counter() - t0
     plain_rate = done / plain_s if plain_s > 0 else None
 
-    step_ms, e2e_ms, rep = _maxr([ms / a.steps, e2e_ms, rep], world)
+    step_ms, e2e_ms, rep, full = _maxr([ms / a.steps, e2e_ms, rep, full], world)
     hbm, src = _peak()
-    achieved = alg_bytes / (rep / 1e3) / 1e9
+    achieved = alg_bytes / (full / 1e3) / 1e9
     line = {
         "metric": "set-intersections/sec (Jaccard 0.7 self-join: prefix-filter candidates "
                   "decided by one graph-captured batch launch)",
@@ -211,12 +230,15 @@ def sss_join_ours(a, rank, world, local):
                    "autotuned": {"alpha": hp.alpha, "bucket": hp.b,
                                  "probe_rounds": hp.probe_rounds,
                                  "warp_pair_min": hp.warp_pair_min},
-                   "step": "prefix-filter candidates + batch replay + pair-list compaction "
-                           "(index resident)",
+                   "step": "prefix-filter candidates + decisions-only batch replay + "
+                           "pair-list compaction (index resident)",
                    "parallelism": f"replicas x{world}",
                    "l2": "token sets + tables larger than L2; no flush"},
         "batch_launch": {"value": world * P / (rep / 1e3), "unit": "intersections/s",
-                         "ms_per_launch": rep},
+                         "ms_per_launch": rep, "mode": "decisions only (early exit)"},
+        "batch_launch_full_sizes": {"value": world * P / (full / 1e3),
+                                    "unit": "intersections/s", "ms_per_launch": full,
+                                    "mode": "every key probed, |A ∩ B| written"},
         "plain_per_call": {"value": plain_rate, "unit": "intersections/s",
                            "calls": len(pick), "pairs": done,
                            "note": "reset_sss once per query set over its candidates"},
@@ -224,7 +246,8 @@ def sss_join_ours(a, rank, world, local):
                 "h2d_bytes_per_step": 4 * (n + 1) + 4 * m, "d2h_bytes_per_step": out_bytes,
                 "ms_per_step": e2e_ms,
                 "note": "host token sets in; index build, candidates, decisions; pair list out"},
-        "roofline": {"bound": "hbm", "kernel": "sss_kernel (batch replay)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "sss_kernel (batch replay, full sizes)",
+                     "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
                      "traffic": None, "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": launches,

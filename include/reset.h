@@ -169,7 +169,10 @@ reset_status reset_tc_count_noalloc(const reset_table *t, const int32_t *d_off,
  * of sets of the table's CSR.  I = |A ∩ B| by probing the smaller set into
  * the larger set's table; U = |A| + |B| - I.
  *   d_flags[p] = U > 0 && den * I >= num * U            (exact, integer)
- * d_inter (optional) receives I.  Replaces set_similarity_search_kernel
+ * d_inter (optional) receives I; without it the call decides only, and a
+ * pair stops probing as soon as its decision is settled (enough hits, or
+ * too many misses for the threshold to be reachable).  Replaces
+ * set_similarity_search_kernel
  * (set-similarity-search/sss.cu:93-154) and SSSBaseline::run_*
  * (baseline/sss/sss.cu:145-251), whose float rule
  * I / (float)U >= thr is available through reset_sss_float. */
@@ -202,6 +205,14 @@ typedef struct reset_batch reset_batch;
 reset_status reset_batch_create(const reset_table *t, const int32_t *d_elems,
                                 int64_t capacity, int32_t num, int32_t den,
                                 reset_batch **out, reset_stream_t stream);
+/* Options of reset_batch_create_ex. */
+#define RESET_BATCH_DECISIONS_ONLY 1 /* flags only: each pair stops as soon as its
+                                        decision is settled; *d_inter is not
+                                        written                                 */
+reset_status reset_batch_create_ex(const reset_table *t, const int32_t *d_elems,
+                                   int64_t capacity, int32_t num, int32_t den,
+                                   int32_t options, reset_batch **out,
+                                   reset_stream_t stream);
 reset_status reset_batch_buffers(reset_batch *b, int32_t **d_pair_a,
                                  int32_t **d_pair_b, uint8_t **d_flags,
                                  int32_t **d_inter);

@@ -101,6 +101,7 @@ SIGNATURES = {
                              C.c_double, I32, C.POINTER(P), C.POINTER(P),
                              C.POINTER(I64), P]),
     "reset_batch_create": (I32, [P, P, I64, I32, I32, C.POINTER(P), P]),
+    "reset_batch_create_ex": (I32, [P, P, I64, I32, I32, I32, C.POINTER(P), P]),
     "reset_batch_buffers": (I32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                   C.POINTER(P)]),
     "reset_batch_run": (I32, [P, I64, P]),

@@ -254,17 +254,20 @@ class Batch:
     """Batched set-similarity decisions over one table (reset_batch_*): a
     captured CUDA graph of the persistent pair kernel with device pair
     buffers for up to `capacity` pairs.  Fill `pair_a` / `pair_b` (views of
-    the batch's own buffers), call run(npairs), read `flags` / `inter`."""
+    the batch's own buffers), call run(npairs), read `flags` / `inter`
+    (`inter` is not written when decisions_only)."""
 
     def __init__(self, t: Table, elems: torch.Tensor, capacity: int, num: int = 7,
-                 den: int = 10, stream=None):
+                 den: int = 10, decisions_only: bool = False, stream=None):
         _need(elems, torch.int32, "elems")
         self._table = t          # the batch reads the table's device arrays
         self._elems = elems
         self.capacity = int(capacity)
+        self.decisions_only = bool(decisions_only)
         h = C.c_void_p()
-        check(_lib().reset_batch_create(t.handle, _ptr(elems), self.capacity, num, den,
-                                        C.byref(h), _stream(stream)))
+        check(_lib().reset_batch_create_ex(t.handle, _ptr(elems), self.capacity, num, den,
+                                           1 if decisions_only else 0, C.byref(h),
+                                           _stream(stream)))
         self._h = h
         pa, pb, fl, it = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
         check(_lib().reset_batch_buffers(h, C.byref(pa), C.byref(pb), C.byref(fl),

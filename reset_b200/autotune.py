@@ -31,7 +31,7 @@ BUCKETS = tuple(range(1, 10))
 class HyperParams:
     alpha: float = 0.2
     b: int = 5
-    probe_rounds: int = 4
+    probe_rounds: int = 8
     warp_pair_min: int = 64
     cost: float = 0.0           # model cost (slot reads per probe) or measured ms
     measured_ms: Optional[float] = None
@@ -143,7 +143,7 @@ def _store(path: str, data: Dict[str, dict]):
 # ----------------------------------------------------------------- solve --
 
 def solve(kind: str, degrees: Sequence[int], measure: Optional[Callable[[HyperParams], float]] = None,
-          measure_top: int = 6, rounds: Sequence[int] = (2, 4),
+          measure_top: int = 6, rounds: Sequence[int] = (4, 8),
           warp_pair_mins: Sequence[int] = (32, 64, 128), cache: Optional[str] = DEFAULT_CACHE,
           alphas: Iterable[float] = ALPHAS, buckets: Iterable[int] = BUCKETS,
           extra_key: str = "",

@@ -17,7 +17,8 @@ reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
                                    const int64_t* np_dev,
                                    unsigned long long* cursor, int64_t capacity,
                                    int32_t num, int32_t den, uint8_t* flags,
-                                   int32_t* inter, cudaStream_t st);
+                                   int32_t* inter, bool decisions_only,
+                                   cudaStream_t st);
 }
 
 struct reset_batch {
@@ -57,6 +58,14 @@ extern "C" {
 reset_status reset_batch_create(const reset_table* t, const int32_t* d_elems,
                                 int64_t capacity, int32_t num, int32_t den,
                                 reset_batch** out, reset_stream_t stream) {
+  return reset_batch_create_ex(t, d_elems, capacity, num, den, 0, out, stream);
+}
+
+reset_status reset_batch_create_ex(const reset_table* t, const int32_t* d_elems,
+                                   int64_t capacity, int32_t num, int32_t den,
+                                   int32_t options, reset_batch** out,
+                                   reset_stream_t stream) {
+  if (options & ~RESET_BATCH_DECISIONS_ONLY) return arg_fail("unknown batch option");
   if (!t || !out) return arg_fail("NULL table or output");
   if (!d_elems && t->m > 0) return arg_fail("NULL elements");
   if (capacity < 1 || capacity > INT32_MAX) return arg_fail("capacity must be in 1..2^31-1");
@@ -88,7 +97,8 @@ reset_status reset_batch_create(const reset_table* t, const int32_t* d_elems,
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     rs = sss_launch_persistent(t, d_elems, b->pa, b->pb, b->np_dev, b->cursor, capacity,
-                               num, den, b->flags, b->inter, cap);
+                               num, den, b->flags, b->inter,
+                               (options & RESET_BATCH_DECISIONS_ONLY) != 0, cap);
     cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
     if (e == cudaSuccess) e = e2;
   }

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 
 // ---------------------------------------------------------------- SSS ----
 
-template <bool HIER, bool FLOAT_RULE, int ROUNDS, bool LEAN>
+template <bool HIER, bool FLOAT_RULE, int ROUNDS, bool LEAN, bool EARLY = false>
 __global__ void __launch_bounds__(kThreads, 4)
     sss_kernel(const int4* __restrict__ desc, int32_t n,
                const int32_t* __restrict__ elems, int64_t n_elems,
@@ -183,11 +183,26 @@ __global__ void __launch_bounds__(kThreads, 4)
       const int ka = __shfl_sync(kFull, A.x, k);
       const int klg = __shfl_sync(kFull, blg, k);
       const int64_t kt = __shfl_sync(kFull, bt, k);
-      int h = LEAN ? warp_probe_pair_lean<HIER, ROUNDS>(elems + ka, ks, table + kt, klg,
-                                                        lg_max, bn, b, status, s_qx[warp],
-                                                        s_qh[warp])
-                   : warp_probe_pair<HIER, ROUNDS>(elems + ka, ks, table + kt, klg, lg_max,
-                                                   bn, b, status, s_qx[warp], s_qh[warp]);
+      int h;
+      if (EARLY) {
+        // decisions only: need = smallest I with den*I >= num*(|A|+|B|-I)
+        const int kd = __shfl_sync(kFull, da.y + dq.y, k);
+        const int64_t need64 = ((int64_t)num * kd + (num + den) - 1) / (num + den);
+        const int need = (int)need64;
+        if (need > ks) {
+          h = 0;  // unreachable: not similar, no probes
+        } else {
+          h = warp_probe_pair_lean<HIER, ROUNDS, true>(elems + ka, ks, table + kt, klg,
+                                                       lg_max, bn, b, status, s_qx[warp],
+                                                       s_qh[warp], need, ks - need);
+        }
+      } else if (LEAN) {
+        h = warp_probe_pair_lean<HIER, ROUNDS>(elems + ka, ks, table + kt, klg, lg_max, bn,
+                                               b, status, s_qx[warp], s_qh[warp]);
+      } else {
+        h = warp_probe_pair<HIER, ROUNDS>(elems + ka, ks, table + kt, klg, lg_max, bn, b,
+                                          status, s_qx[warp], s_qh[warp]);
+      }
       h = __reduce_add_sync(kFull, h);
       if (lane == 0) s_hits[warp][k] += h;
       __syncwarp();
@@ -502,23 +517,26 @@ reset_status sss_launch_persistent(const reset_table* t, const int32_t* elems,
                                    const int64_t* np_dev,
                                    unsigned long long* cursor, int64_t capacity,
                                    int32_t num, int32_t den, uint8_t* flags,
-                                   int32_t* inter, cudaStream_t st) {
+                                   int32_t* inter, bool decisions_only,
+                                   cudaStream_t st) {
   const reset_tuning tun = tuning();
   const int wpm = tun.warp_pair_min;
-#define SSS_P(H, R, LN)                                                        \
+#define SSS_P(H, R, LN, E)                                                     \
   do {                                                                         \
     const int64_t g = clamp_grid(((capacity + 31) / 32 + kWarps - 1) / kWarps, \
-                                 persistent_grid((const void*)sss_kernel<H, false, R, LN>)); \
+                                 persistent_grid((const void*)sss_kernel<H, false, R, LN, E>)); \
     note_launch();                                                             \
-    sss_kernel<H, false, R, LN><<<(int)g, kThreads, 0, st>>>(                  \
+    sss_kernel<H, false, R, LN, E><<<(int)g, kThreads, 0, st>>>(               \
         t->d_desc, t->n, elems, t->m, pa, pb, capacity, np_dev, cursor,        \
         t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, 0.f, wpm,   \
-        flags, inter, t->d_status);                                            \
+        flags, E ? nullptr : inter, t->d_status);                              \
   } while (0)
-  if (tun.probe_variant == 1) {
-    if (t->hier) SSS_P(true, 8, true); else SSS_P(false, 8, true);
+  if (decisions_only) {
+    if (t->hier) SSS_P(true, 8, true, true); else SSS_P(false, 8, true, true);
+  } else if (tun.probe_variant == 1) {
+    if (t->hier) SSS_P(true, 8, true, false); else SSS_P(false, 8, true, false);
   } else {
-    if (t->hier) SSS_P(true, 4, false); else SSS_P(false, 4, false);
+    if (t->hier) SSS_P(true, 4, false, false); else SSS_P(false, 4, false, false);
   }
 #undef SSS_P
   RST_CUDA(cudaGetLastError());
@@ -638,11 +656,11 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   DescScope ds;
   RST_CHECK(resolve_desc(t, d_off, st, &ds));
   const reset_tuning tun = tuning();
-#define SSS_LAUNCH(H, F, R, LN)                                              \
+#define SSS_LAUNCH(H, F, R, LN, ...)                                         \
   do {                                                                       \
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \
-                                 persistent_grid((const void*)sss_kernel<H, F, R, LN>)); \
-    note_launch(); sss_kernel<H, F, R, LN><<<(int)g, kThreads, 0, st>>>(      \
+                                 persistent_grid((const void*)sss_kernel<H, F, R, LN, ##__VA_ARGS__>)); \
+    note_launch(); sss_kernel<H, F, R, LN, ##__VA_ARGS__><<<(int)g, kThreads, 0, st>>>( \
         ds.desc, t->n, d_elems, t->m, d_pa, d_pb, np, nullptr, nullptr,      \
         t->d_table, t->bucket_num, t->bucket, t->lg_max, num, den, thr,       \
         tun.warp_pair_min, d_flags, d_inter, t->d_status);                    \
@@ -652,7 +670,11 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
     if (tun.probe_variant == 1) SSS_LAUNCH(H, F, 8, true);                   \
     else SSS_LAUNCH(H, F, 4, false);                                         \
   } while (0)
-  if (t->hier) {
+  if (!float_rule && !d_inter) {
+    // decisions only: pairs stop as soon as the rule is settled
+    if (t->hier) SSS_LAUNCH(true, false, 8, true, true);
+    else SSS_LAUNCH(false, false, 8, true, true);
+  } else if (t->hier) {
     if (float_rule) SSS_V(true, true); else SSS_V(true, false);
   } else {
     if (float_rule) SSS_V(false, true); else SSS_V(false, false);

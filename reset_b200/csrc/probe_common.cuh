@@ -226,13 +226,18 @@ __device__ __forceinline__ int warp_probe_pair(const int32_t* __restrict__ keys,
 // shared-memory queue (qx/qh, 32*R entries), walked together after the
 // batch.  No prefetch across batches: latency is hidden by the other
 // resident warps.  Returns this lane's hits.
-template <bool HIER, int R>
+//
+// EARLY (decisions only): after every batch the warp totals its hits and
+// stops once they reach need_hits or once its misses exceed max_miss; the
+// partial total then decides a threshold rule exactly as the full one would.
+template <bool HIER, int R, bool EARLY = false>
 __device__ __forceinline__ int warp_probe_pair_lean(const int32_t* __restrict__ keys,
                                                     int s,
                                                     const int32_t* __restrict__ tb,
                                                     int lg, int lg_max, int64_t bn,
                                                     int b, int32_t* status,
-                                                    int* qx, int* qh) {
+                                                    int* qx, int* qh,
+                                                    int need_hits = 0, int max_miss = 0) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int32_t* __restrict__ tb1 = tb + (b > 1 ? bn : 0);
@@ -280,6 +285,11 @@ __device__ __forceinline__ int warp_probe_pair_lean(const int32_t* __restrict__ 
       for (int i = lane; i < nq; i += 32)
         hits += probe_walk<HIER>(qx[i], tb, lg, qh[i], k0, bn, b, status);
       __syncwarp();
+    }
+    if (EARLY) {
+      const int tot = __reduce_add_sync(kFull, hits);
+      const int done = min(base + 32 * R, s);
+      if (tot >= need_hits || done - tot > max_miss) return lane == 0 ? tot : 0;
     }
   }
   return hits;

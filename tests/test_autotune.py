@@ -31,7 +31,7 @@ def test_solve_picks_the_fastest_measurement_and_caches(tmp_path):
     cache = str(tmp_path / "tune.json")
     hp = A.solve("sss", degs, measure=fake_ms, measure_top=3, cache=cache)
     assert (hp.alpha, hp.b, hp.warp_pair_min) == (0.2, 5, 128)
-    assert (0.2, 5, 4, 64) in seen          # the reference default is always measured
+    assert (0.2, 5) in {(a, b) for a, b, _, _ in seen}   # the reference default is measured
     n = len(seen)
     hp2 = A.solve("sss", degs, measure=fake_ms, cache=cache)
     assert len(seen) == n and hp2 == hp      # served from the cache

@@ -118,6 +118,35 @@ def test_batch_equals_sss_across_replays(R, oracle_mod, cuda):
     batch.close()
 
 
+@pytest.mark.parametrize("num,den", [(7, 10), (1, 4), (0, 1), (1, 1), (9, 10)])
+def test_decisions_only_equal_full_decisions(R, oracle_mod, cuda, num, den):
+    """Early exit (no intersection sizes wanted) decides exactly as the full
+    probe: plain call without d_inter, and a decisions-only batch."""
+    torch = cuda
+    off, tok = R.gen_token_sets(30000, 16, 1.2, 8, 600, seed=0x5EED4000, dup_frac=0.4,
+                                keep_min=0.6)
+    t = R.Table(off, tok, hierarchical=True)
+    pa, pb = R.prefix_candidates(off, tok, 16, 7, 10)
+    g = torch.Generator(device="cuda").manual_seed(9)
+    n = off.numel() - 1
+    ra = torch.randint(0, n, (50000,), device="cuda", dtype=torch.int32, generator=g)
+    rb = torch.randint(0, n, (50000,), device="cuda", dtype=torch.int32, generator=g)
+    pa, pb = torch.cat([pa, ra, pa]), torch.cat([pb, rb, pa])   # similar, random, self pairs
+    full, _ = R.sss(t, off, tok, pa, pb, num, den)
+    dec, none = R.sss(t, off, tok, pa, pb, num, den, with_inter=False)
+    assert none is None and torch.equal(full, dec)
+    assert int(full.sum()) > 0
+    b = R.Batch(t, tok, capacity=pa.numel(), num=num, den=den, decisions_only=True)
+    f, _ = b(pa, pb)
+    assert torch.equal(f, full)
+    b.close()
+    if num == 7:
+        sub = slice(0, 40000)
+        of, _ = oracle_mod.sss(oracle_mod.Table(host(off), host(tok), hier=1),
+                               host(pa[sub]), host(pb[sub]), mode=1, num=num, den=den)
+        assert np.array_equal(host(dec[sub]), of.astype(np.uint8))
+
+
 def test_batch_replays_queue_without_host_sync(R, cuda):
     """Back-to-back runs of different sizes on one stream, read at the end:
     each replay sees its own pair count."""
