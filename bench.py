@@ -311,7 +311,7 @@ def run_ours(a, rank, world, local):
     achieved = alg_bytes / (probe_avg / 1e3) / 1e9
     traffic = None
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_kernel_traffic.json")))
+        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_kernel_rmat_s20_traffic.json")))
         if prof.get("scale") == a.scale:
             traffic = prof.get("dram_bytes_per_launch")
     except Exception:
