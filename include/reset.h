@@ -106,6 +106,11 @@ reset_status reset_table_info(const reset_table *t, reset_table_view *view);
  * pages mapped, so the next build of a similar table maps no new memory. */
 reset_status reset_table_free(reset_table *t);
 
+/* Stream-ordered free: the table's memory returns to the pool when `stream`
+ * reaches this point; no host or device synchronisation.  Every use of the
+ * table on other streams must be ordered before it (events) by the caller. */
+reset_status reset_table_free_async(reset_table *t, reset_stream_t stream);
+
 /* Returns the pages the table pool keeps for reuse to the device
  * (no counterpart in the reference).  Synchronises the device. */
 reset_status reset_release_cached_memory(void);

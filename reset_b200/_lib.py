@@ -87,6 +87,7 @@ SIGNATURES = {
                                 C.POINTER(P), P]),
     "reset_table_info": (I32, [P, C.POINTER(TableView)]),
     "reset_table_free": (I32, [P]),
+    "reset_table_free_async": (I32, [P, P]),
     "reset_release_cached_memory": (I32, []),
     "reset_table_check": (I32, [P, P]),
     "reset_csr_hash_order": (I32, [P, P, P, P]),

@@ -122,6 +122,13 @@ class Table:
             check(_lib().reset_table_free(self._h))
             self._h = None
 
+    def free_async(self, stream=None):
+        """Stream-ordered free (reset_table_free_async): every use of the
+        table must be ordered before this point of `stream`."""
+        if self._h is not None:
+            check(_lib().reset_table_free_async(self._h, _stream(stream)))
+            self._h = None
+
     def __del__(self):
         try:
             if getattr(self, "_h", None) is not None:

@@ -762,6 +762,22 @@ reset_status reset_table_free(reset_table* t) {
   return RESET_OK;
 }
 
+reset_status reset_table_free_async(reset_table* t, reset_stream_t stream) {
+  if (!t) return RESET_OK;
+  cudaStream_t st = as_stream(stream);
+  void* ptrs[] = {t->d_table, t->d_len, t->d_off64, t->d_desc, t->d_chunk_row,
+                  t->d_status};
+  cudaError_t e = cudaSuccess;
+  for (void* p : ptrs)
+    if (p) {
+      cudaError_t e2 = cudaFreeAsync(p, st);
+      if (e == cudaSuccess) e = e2;
+    }
+  delete t;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync", __FILE__, __LINE__);
+  return RESET_OK;
+}
+
 reset_status reset_release_cached_memory(void) {
   RST_CUDA(cudaDeviceSynchronize());
   release_pools();
