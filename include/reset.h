@@ -255,6 +255,17 @@ reset_status reset_ir(const reset_table *t, const int32_t *d_toff,
                       const int64_t *d_res_off, int32_t *d_res,
                       int32_t *d_cnt, reset_stream_t stream);
 
+/* 4-cliques of an oriented graph (rows sorted ascending, oriented as for
+ * reset_tc_count) whose table is `t` (built on d_off/d_cols):
+ *   sum over edges (u, v) of sum over w in W of |W ∩ N+(w)|,
+ * W = N+(u) ∩ N+(v), every intersection by hash probes.  *d_count (device
+ * u64) is overwritten.  The depth-4 clique search of SMOG's
+ * DFSKernelForClique (SMOG/SMOG_hie/subgraph_match_hie.cu:58-247) over this
+ * library's tables.  Synchronises `stream` once (scratch sizing). */
+reset_status reset_clique4_count(const reset_table *t, const int32_t *d_off,
+                                 const int32_t *d_cols, int64_t m,
+                                 uint64_t *d_count, reset_stream_t stream);
+
 /* |A ∩ B| counted with A's multiplicity for one pair of device arrays
  * (keys >= 0).  Builds B's table with `params` and probes A.  *d_count
  * (device i64) is overwritten.  Replaces make_hashtable_kernel +

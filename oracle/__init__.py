@@ -84,6 +84,8 @@ def lib():
         L.ro_jaccard_join.argtypes = [C.c_int32, _i32p, _i32p, C.c_int32,
                                       C.c_int32, _i32p, _i32p, C.c_int64]
         L.ro_jaccard_join.restype = C.c_int64
+        L.ro_clique4.argtypes = [C.c_int32, _i32p, _i32p]
+        L.ro_clique4.restype = C.c_uint64
         L.ro_relabel.argtypes = [C.c_uint64, C.c_int32, C.c_uint32]
         L.ro_relabel.restype = C.c_uint32
         L.ro_mix64.argtypes = [C.c_uint64]
@@ -210,6 +212,13 @@ def pair_count(a, b) -> int:
     b = _c(b, np.int32)
     return int(lib().ro_pair_count(a if a.size else np.zeros(1, np.int32), a.size,
                                    b if b.size else np.zeros(1, np.int32), b.size))
+
+
+def clique4(off, cols) -> int:
+    """4-cliques of an oriented graph with sorted rows."""
+    off = _c(off, np.int32)
+    cols = _c(cols, np.int32)
+    return int(lib().ro_clique4(off.size - 1, off, cols if cols.size else np.zeros(1, np.int32)))
 
 
 def jaccard_join(off, tok, num=7, den=10):

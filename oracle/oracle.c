@@ -414,6 +414,41 @@ int64_t ro_jaccard_join(int32_t n, const int32_t *off, const int32_t *tok,
   return k;
 }
 
+/* 4-cliques of an oriented graph with sorted rows: for every edge (u, v),
+ * W = N+(u) ∩ N+(v) by merging, then for every w in W, |W ∩ N+(w)| by
+ * merging (each 4-clique counted once from its two lowest vertices; the
+ * multi-way intersections of SMOG/SMOG_hie/subgraph_match_hie.cu:58-247 at
+ * depth 4).  Test sizes only. */
+uint64_t ro_clique4(int32_t n, const int32_t *off, const int32_t *cols) {
+  int32_t maxd = 0;
+  for (int32_t u = 0; u < n; u++)
+    if (off[u + 1] - off[u] > maxd) maxd = off[u + 1] - off[u];
+  int32_t *W = (int32_t *)malloc(sizeof(int32_t) * (size_t)(maxd > 0 ? maxd : 1));
+  uint64_t total = 0;
+  for (int32_t u = 0; u < n; u++) {
+    for (int32_t e = off[u]; e < off[u + 1]; e++) {
+      const int32_t v = cols[e];
+      int32_t i = off[u], j = off[v], nw = 0;
+      while (i < off[u + 1] && j < off[v + 1]) {
+        if (cols[i] < cols[j]) i++;
+        else if (cols[i] > cols[j]) j++;
+        else { W[nw++] = cols[i]; i++; j++; }
+      }
+      for (int32_t t = 0; t < nw; t++) {
+        const int32_t w = W[t];
+        int32_t a = 0, b = off[w];
+        while (a < nw && b < off[w + 1]) {
+          if (W[a] < cols[b]) a++;
+          else if (W[a] > cols[b]) b++;
+          else { total++; a++; b++; }
+        }
+      }
+    }
+  }
+  free(W);
+  return total;
+}
+
 /* ------------------------------------------------------------------------ */
 /* synthetic inputs                                                          */
 /* ------------------------------------------------------------------------ */

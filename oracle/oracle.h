@@ -112,6 +112,9 @@ int64_t ro_jaccard_join(int32_t n, const int32_t *off, const int32_t *tok,
                         int32_t num, int32_t den, int32_t *pa, int32_t *pb,
                         int64_t cap);
 
+/* 4-cliques of an oriented graph with sorted rows (merge intersections). */
+uint64_t ro_clique4(int32_t n, const int32_t *off, const int32_t *cols);
+
 /* ---- synthetic inputs --------------------------------------------------- */
 
 /* splitmix64 finaliser; the R-MAT draw for edge i uses 16-bit fields of

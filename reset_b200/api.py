@@ -158,6 +158,14 @@ def tc_count(t: Table, off: torch.Tensor, cols: torch.Tensor, method: int = TC_D
     return int(out.item()) & ((1 << 64) - 1)
 
 
+def clique4_count(t: Table, off: torch.Tensor, cols: torch.Tensor, stream=None) -> int:
+    """4-cliques of the oriented graph the table was built on."""
+    out = torch.zeros(1, dtype=torch.int64, device=cols.device)
+    check(_lib().reset_clique4_count(t.handle, _ptr(off), _ptr(cols), cols.numel(), _ptr(out),
+                                     _stream(stream)))
+    return int(out.item()) & ((1 << 64) - 1)
+
+
 def sss(t: Table, off, elems, pa, pb, num: int = 7, den: int = 10,
         with_inter: bool = True, stream=None):
     """Integer-rule set-similarity decisions -> (flags uint8, inter int32)."""

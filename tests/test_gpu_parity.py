@@ -347,3 +347,50 @@ def test_every_probe_variant_counts_the_same(R, cuda, oracle_mod, variant, round
     finally:
         R.set_tuning(probe_rounds=4, probe_variant=before["probe_variant"])
         R.set_tuning(**before)
+
+
+def test_free_async_across_streams(R, cuda, oracle_mod):
+    """Build on one stream, count on another, free stream-ordered on the
+    counting stream; repeated back to back without host syncs."""
+    torch = cuda
+    off, cols = R.gen_rmat(14, 16, 0x5EED7100, oriented=True)
+    want = oracle_mod.tc_merge(host(off), host(cols))
+    s_build, s_probe = torch.cuda.Stream(), torch.cuda.Stream()
+    outs = []
+    for _ in range(6):
+        with torch.cuda.stream(s_build):
+            t = R.Table(off, cols, hierarchical=True, hash_order=True, stream=s_build)
+            ev = torch.cuda.Event()
+            ev.record(s_build)
+        s_probe.wait_event(ev)
+        with torch.cuda.stream(s_probe):
+            c = R.tc_count_async(t, off, t.hash_order, stream=s_probe)
+        t.hash_order.record_stream(s_probe)
+        t.free_async(s_probe)
+        outs.append(c)
+    torch.cuda.synchronize()
+    assert [int(c.item()) for c in outs] == [want] * 6
+
+
+# ------------------------------------------------------------ 4-cliques --
+
+@pytest.mark.parametrize("scale,hier", [(8, True), (11, True), (11, False), (14, True)])
+def test_clique4_matches_oracle(R, cuda, oracle_mod, scale, hier):
+    off, cols = R.gen_rmat(scale, 16, 0x5EED4C00 + scale, oriented=True)
+    want = oracle_mod.clique4(host(off), host(cols))
+    t = R.Table(off, cols, hierarchical=hier)
+    assert R.clique4_count(t, off, cols) == want
+    t.check()
+
+
+def test_clique4_complete_graph(R, cuda):
+    torch = cuda
+    from math import comb
+    n = 40
+    rows = [list(range(u + 1, n)) for u in range(n)]
+    off = np.zeros(n + 1, np.int32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    cols = np.array(sum(rows, []), np.int32)
+    d_off, d_cols = dev(off, torch), dev(cols, torch)
+    t = R.Table(d_off, d_cols)
+    assert R.clique4_count(t, d_off, d_cols) == comb(n, 4)

@@ -256,3 +256,23 @@ def test_prefix_filter_keeps_every_join_pair(oracle_mod):
         for a, b in list(zip(ja.tolist(), jb.tolist()))[:20]:
             A, B = set(rows[a].tolist()), set(rows[b].tolist())
             assert den * len(A & B) >= num * len(A | B)
+
+
+def test_clique4_oracle_small_cases(oracle_mod):
+    from math import comb
+    for n in (3, 4, 7, 12):
+        rows = [list(range(u + 1, n)) for u in range(n)]
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum([len(r) for r in rows])
+        cols = np.array(sum(rows, []), np.int32)
+        assert oracle_mod.clique4(off, cols) == comb(n, 4)
+    # brute force on a small R-MAT graph
+    off, cols = oracle_mod.rmat_graph(7, 8, 3, oriented=True)
+    n = off.size - 1
+    adj = [set(cols[off[u]:off[u + 1]].tolist()) for u in range(n)]
+    want = 0
+    for a in range(n):
+        for b in adj[a]:
+            for c in adj[a] & adj[b]:
+                want += len(adj[a] & adj[b] & adj[c])
+    assert oracle_mod.clique4(off, cols) == want
