@@ -317,9 +317,13 @@ def test_tc_methods_agree_rmat(R, cuda, oracle_mod, scale):
 
 # --------------------------------------------------------- tuning knobs --
 
-@pytest.mark.parametrize("variant,rounds,wpm", [(0, 2, 64), (0, 4, 1), (1, 2, 32), (1, 4, 64),
-                                                (1, 8, 64), (1, 8, 1), (1, 8, 100000)])
-def test_every_probe_variant_counts_the_same(R, cuda, oracle_mod, variant, rounds, wpm):
+@pytest.mark.parametrize("variant,rounds,wpm,alpha,bucket", [
+    (0, 2, 64, 0.2, 5), (0, 4, 1, 0.2, 5), (1, 2, 32, 0.2, 5), (1, 4, 64, 0.2, 5),
+    (1, 8, 64, 0.2, 5), (1, 8, 1, 0.2, 5), (1, 8, 100000, 0.2, 5),
+    (1, 8, 64, 0.4, 2), (1, 8, 1, 0.4, 2), (1, 8, 64, 0.25, 1), (1, 4, 32, 0.9, 1),
+    (1, 8, 64, 1.0, 2), (0, 4, 64, 0.4, 2)])
+def test_every_probe_variant_counts_the_same(R, cuda, oracle_mod, variant, rounds, wpm,
+                                             alpha, bucket):
     """The probe knobs change scheduling only: TC counts, SSS flags and sizes
     equal the oracle for every variant, both hashes."""
     torch = cuda
@@ -331,7 +335,8 @@ def test_every_probe_variant_counts_the_same(R, cuda, oracle_mod, variant, round
         off, cols = R.gen_rmat(13, 16, 0x5EED7000, oriented=True)
         want = oracle_mod.tc_merge(host(off), host(cols))
         for hier in (True, False):
-            t = R.Table(off, cols, hierarchical=hier, hash_order=True)
+            t = R.Table(off, cols, alpha=alpha, bucket=bucket, hierarchical=hier,
+                        hash_order=True)
             assert R.tc_count(t, off, t.hash_order) == want
             assert R.tc_count(t, off, cols) == want
         s_off, s_cols = R.gen_rmat(11, 16, 0x5EED7001, oriented=False)
