@@ -72,3 +72,35 @@ def test_no_oracle_in_product():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 txt = open(os.path.join(dp, f)).read()
                 assert "import oracle" not in txt and "liboracle" not in txt, f
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors have the C layout: sizes and every field offset,
+    printed by a C program compiled against include/reset.h."""
+    import subprocess
+    from reset_b200 import _lib
+    structs = {"reset_params": _lib.Params, "reset_tuning": _lib.Tuning,
+               "reset_table_view": _lib.TableView, "reset_server_config": _lib.ServerConfig,
+               "reset_request": _lib.Request, "reset_result": _lib.Result,
+               "reset_server_counters": _lib.ServerCounters}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "reset.h"',
+             'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append('  return 0; }')
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    got = {}
+    for line in out.splitlines():
+        cname, key, val = line.split()
+        got[(cname, key)] = int(val)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
