@@ -7,6 +7,7 @@
  *   reset::TCBaseline                       <- baseline/tc/tc.cuh:15-59
  *   reset::SSSBaseline                      <- baseline/sss/sss.cuh:12-69
  *   reset::IRBaseline                       <- baseline/ir/ir.cuh:13-87
+ * and wraps the batched and served forms (reset::Batch, reset::Server).
  * Same names, argument meaning and return values (pairs of result and
  * kernel milliseconds).  Launch-shape arguments of the reference (CHUNK_SIZE,
  * grid_size, block_size) are accepted and ignored: the library sizes its own
@@ -339,6 +340,107 @@ class IRBaseline : public HashTableBuilder {
   int nq_ = 0;
   DeviceBuffer<int> d_q_, d_qoff_, d_res_, d_cnt_;
   DeviceBuffer<int64_t> d_roff_;
+};
+
+// ---- forms with no counterpart in the reference ---------------------------
+
+// Batched pair decisions over one table (reset_batch_*): fill pair_a()/pair_b()
+// on the device, run(np), read flags()/inter().
+class Batch {
+ public:
+  Batch(const reset_table* t, const int32_t* d_elems, int64_t capacity, int num = 7,
+        int den = 10, bool decisions_only = false, cudaStream_t stream = nullptr) {
+    check(reset_batch_create_ex(t, d_elems, capacity, num, den,
+                                decisions_only ? RESET_BATCH_DECISIONS_ONLY : 0, &b_,
+                                stream));
+    check(reset_batch_buffers(b_, &pa_, &pb_, &flags_, &inter_));
+  }
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+  ~Batch() { reset_batch_destroy(b_); }
+  int32_t* pair_a() const { return pa_; }
+  int32_t* pair_b() const { return pb_; }
+  uint8_t* flags() const { return flags_; }
+  int32_t* inter() const { return inter_; }
+  void run(int64_t np, cudaStream_t stream = nullptr) { check(reset_batch_run(b_, np, stream)); }
+
+ private:
+  reset_batch* b_ = nullptr;
+  int32_t *pa_ = nullptr, *pb_ = nullptr, *inter_ = nullptr;
+  uint8_t* flags_ = nullptr;
+};
+
+// A result of the served form, copied out of the server.
+struct ServedResult {
+  reset_status status = RESET_OK;
+  int64_t count = 0;
+  std::vector<int32_t> docs;
+  std::vector<int64_t> values;
+  std::vector<uint8_t> flags;
+  double queue_us = 0, service_us = 0, latency_us = 0;
+  int32_t batch_size = 0;
+};
+
+// The served form (reset_server_*): submit() returns at once, wait() blocks.
+class Server {
+ public:
+  explicit Server(int streams = 4, int max_batch_requests = 1024, int64_t mem_budget = 0) {
+    reset_server_config cfg;
+    reset_server_config_default(&cfg);
+    cfg.streams = streams;
+    cfg.max_batch_requests = max_batch_requests;
+    cfg.mem_budget_bytes = mem_budget;
+    check(reset_server_create(&cfg, &s_));
+  }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  ~Server() { reset_server_destroy(s_); }
+  int add_index(const reset_table* t, const int32_t* d_off, const int32_t* d_elems) {
+    int32_t ix = 0;
+    check(reset_server_add_index(s_, t, d_off, d_elems, &ix));
+    return ix;
+  }
+  uint64_t submit(int kind, int index, const int32_t* args, int64_t nargs,
+                  const int32_t* args2 = nullptr, int64_t nargs2 = 0, int num = 7,
+                  int den = 10, int64_t arrival_ns = 0) {
+    reset_request q = {};
+    q.kind = kind;
+    q.index = index;
+    q.args = args;
+    q.nargs = nargs;
+    q.args2 = args2;
+    q.nargs2 = nargs2;
+    q.num = num;
+    q.den = den;
+    q.arrival_ns = arrival_ns;
+    uint64_t t = 0;
+    check(reset_server_submit(s_, &q, &t));
+    return t;
+  }
+  ServedResult wait(uint64_t ticket, int timeout_ms = -1) {
+    reset_result r;
+    check(reset_server_wait(s_, ticket, timeout_ms, &r));
+    ServedResult out;
+    out.status = r.status;
+    out.count = r.count;
+    if (r.ndocs) out.docs.assign(r.docs, r.docs + r.ndocs);
+    if (r.nvalues) out.values.assign(r.values, r.values + r.nvalues);
+    if (r.nvalues && r.flags) out.flags.assign(r.flags, r.flags + r.nvalues);
+    out.queue_us = r.queue_us;
+    out.service_us = r.service_us;
+    out.latency_us = r.latency_us;
+    out.batch_size = r.batch_size;
+    check(reset_server_release(s_, ticket));
+    return out;
+  }
+  reset_server_counters stats() {
+    reset_server_counters c;
+    check(reset_server_stats(s_, &c));
+    return c;
+  }
+
+ private:
+  reset_server* s_ = nullptr;
 };
 
 }  // namespace reset

@@ -83,6 +83,12 @@ def test_reset_ir_cli(cuda, libreset, tmp_path):
     out = run("reset_ir", d)
     got = int(re.search(r"Total result count: (\d+)", out).group(1))
     assert got == int(g["ref_count_normal"].sum()) == int(g["ref_count_hier"].sum())
+    # the same queries through the native serving driver, burst and Poisson
+    for extra in ([], ["--rate=20000", "--streams=2", "--max-batch=8"]):
+        out = run("reset_serve_ir", d, *extra)
+        served = int(re.search(r"Total result count: (\d+)", out).group(1))
+        assert served == got
+        assert re.search(r"served: [0-9.]+ queries/s, latency p50", out)
 
 
 @pytest.mark.parametrize("name", ["pair_1000_3000", "pair_4096_4096", "pair_17_100"])
