@@ -293,17 +293,26 @@ def _ir_queries(df, nq, rng):
     return out
 
 
-def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None):
-    """Submits `reqs` (all at once, or Poisson at `rate`/s for `seconds`),
-    waits for all; returns (results, wall seconds, list of requests used)."""
+def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None, window=4096):
+    """Submits `reqs` closed-loop with at most `window` outstanding (rate
+    None: capacity), or Poisson at `rate`/s for `seconds`; waits for all;
+    returns (results, wall seconds, list of requests used)."""
+    from collections import deque
     from reset_b200.server import now_ns
     tickets = []
     used = []
     t0 = time.perf_counter()
     if rate is None:
+        res = []
+        pend = deque()
         for q in reqs:
-            tickets.append(submit(q, 0))
+            if len(pend) >= window:
+                res.append(srv.wait(pend.popleft()))
+            pend.append(submit(q, 0))
             used.append(q)
+        while pend:
+            res.append(srv.wait(pend.popleft()))
+        return res, time.perf_counter() - t0, used
     else:
         base = now_ns() + 2_000_000
         t = 0.0
@@ -417,6 +426,7 @@ def ir_serve_ours(a, rank, world, local):
                    "mean_terms": qterms, "burst_requests": a.requests,
                    "streams": a.streams, "max_batch": a.max_batch,
                    "mean_batch_in_burst": st["mean_batch"],
+                   "capacity_client": "closed loop, 4096 requests outstanding",
                    "server_counters_after_burst": st,
                    "results_checked_exactly": checked[0],
                    "parallelism": f"replicas x{world}"},

@@ -178,6 +178,18 @@ struct Index {
   int32_t n() const { return (int32_t)h_off.size() - 1; }
 };
 
+// A pinned host block holding the IR survivors of one batch; requests keep
+// it alive (shared ownership) until they are released, so results are
+// handed out without copying.  Blocks are reused from the server's pool.
+struct PinnedBlock {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~PinnedBlock() {
+    if (p) cudaFreeHost(p);
+  }
+};
+using BlockP = std::shared_ptr<PinnedBlock>;
+
 struct Req {
   uint64_t id = 0;
   int32_t kind = 0, index = 0, num = 7, den = 10;
@@ -186,7 +198,8 @@ struct Req {
   int64_t dev_bytes = 0;
   int64_t aux = 0;  // IR: df(first term); TC: number of (v, w) pairs; RAW: len
   reset_status status = RESET_OK;
-  std::vector<int32_t> docs;
+  BlockP docs_block;               // IR: survivors live in this pinned block
+  const int32_t* docs = nullptr;
   std::vector<int64_t> values;
   std::vector<uint8_t> flags;
   int64_t count = 0;
@@ -220,6 +233,7 @@ struct Pinned {
   }
 };
 
+
 struct Group {
   int32_t kind = 0, index = 0, num = 0, den = 0;
   std::vector<Req*> reqs;
@@ -243,13 +257,14 @@ struct Batch {
   int64_t reserved = 0;
   int64_t t_launch = 0;
   int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
+  BlockP res;     // pinned block receiving the IR survivors (phase 1)
   reset_status status = RESET_OK;
 };
 
 struct Slot {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
-  Pinned in, out, res;
+  Pinned in, out;
   void* arena = nullptr;  // device buffer reused by this slot's batches
   size_t arena_cap = 0;
   std::unique_ptr<Batch> batch;  // set while in flight
@@ -275,6 +290,7 @@ struct reset_server {
   int64_t n_done = 0, n_batches = 0, sum_batch = 0, max_batch = 0;
   int64_t max_in_use = 0, max_inflight = 0, inflight = 0;
   int64_t launch_ns = 0, batch_ns = 0;
+  std::vector<BlockP> blocks;  // pinned result blocks (free when only the pool holds one)
 };
 
 namespace {
@@ -663,9 +679,9 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
       case RESET_REQ_IR: {
         const int32_t c = reinterpret_cast<const int32_t*>(at(g.out[0]))[r->item0];
         const int64_t o = reinterpret_cast<const int64_t*>(at(g.out[1]))[r->item0];
-        const int32_t* res = static_cast<const int32_t*>(sl.res.p) + g.dense_host + o;
         r->count = c;
-        r->docs.assign(res, res + c);
+        r->docs_block = c > 0 ? bt.res : nullptr;
+        r->docs = c > 0 ? static_cast<const int32_t*>(bt.res->p) + g.dense_host + o : nullptr;
         break;
       }
       case RESET_REQ_PAIRS: {
@@ -720,7 +736,23 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
 // After the kernels: copies every IR group's packed survivors (sizes now
 // known on the host) into the slot's pinned result buffer.  Returns true if
 // copies were enqueued (the batch completes at the next event).
-bool enqueue_results(Slot& sl, Batch& bt) {
+// A free pinned block of at least `bytes` from the pool (under the server
+// lock), or a new one.
+BlockP take_block(reset_server* s, size_t bytes) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  BlockP best;
+  for (auto& b : s->blocks)
+    if (b.use_count() == 1 && b->cap >= bytes && (!best || b->cap < best->cap)) best = b;
+  if (best) return best;
+  auto b = std::make_shared<PinnedBlock>();
+  const size_t cap = std::max(bytes, (size_t)(1u << 20));
+  if (cudaHostAlloc(&b->p, cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+  b->cap = cap;
+  s->blocks.push_back(b);
+  return b;
+}
+
+bool enqueue_results(reset_server* s, Slot& sl, Batch& bt) {
   const char* hp = static_cast<const char*>(sl.out.p);
   size_t total = 0;
   for (auto& g : bt.groups) {
@@ -730,14 +762,15 @@ bool enqueue_results(Slot& sl, Batch& bt) {
     total += (size_t)g.dense_n;
   }
   if (total == 0) return false;
-  if (sl.res.ensure(4 * total) != cudaSuccess) {
+  bt.res = take_block(s, 4 * total);
+  if (!bt.res) {
     bt.status = cuda_fail(cudaErrorMemoryAllocation, "pinned result buffer", __FILE__, __LINE__);
     return false;
   }
   const char* dp = static_cast<const char*>(bt.d_buf);
   for (auto& g : bt.groups) {
     if (g.kind != RESET_REQ_IR || g.dense_n == 0) continue;
-    cudaError_t e = cudaMemcpyAsync(static_cast<int32_t*>(sl.res.p) + g.dense_host,
+    cudaError_t e = cudaMemcpyAsync(static_cast<int32_t*>(bt.res->p) + g.dense_host,
                                     dp + g.sc[2], 4 * (size_t)g.dense_n,
                                     cudaMemcpyDeviceToHost, sl.st);
     if (e != cudaSuccess) {
@@ -767,7 +800,7 @@ void worker_main(reset_server* s) {
       std::unique_ptr<Batch> bt = std::move(sl.batch);
       lk.unlock();
       if (q != cudaSuccess) bt->status = cuda_fail(q, "server batch", __FILE__, __LINE__);
-      if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(sl, *bt)) {
+      if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(s, sl, *bt)) {
         lk.lock();
         sl.batch = std::move(bt);  // survivors in flight
         progressed = true;
@@ -982,8 +1015,8 @@ reset_status reset_server_wait(reset_server* s, uint64_t ticket, int32_t timeout
   out->status = r->status;
   out->kind = r->kind;
   out->count = r->count;
-  out->docs = r->docs.empty() ? nullptr : r->docs.data();
-  out->ndocs = (int64_t)r->docs.size();
+  out->docs = r->docs;
+  out->ndocs = r->docs ? r->count : 0;
   out->values = r->values.empty() ? nullptr : r->values.data();
   out->nvalues = (int64_t)r->values.size();
   out->flags = r->flags.empty() ? nullptr : r->flags.data();
@@ -1046,8 +1079,9 @@ reset_status reset_server_destroy(reset_server* s) {
     if (sl.arena) cudaFree(sl.arena);
     sl.in.release();
     sl.out.release();
-    sl.res.release();
   }
+  s->reqs.clear();
+  s->blocks.clear();
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   if (e != cudaSuccess) return cuda_fail(e, "reset_server_destroy", __FILE__, __LINE__);
