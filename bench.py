@@ -376,9 +376,11 @@ def run_ours(a, rank, world, local):
     achieved = alg_bytes / (probe_avg / 1e3) / 1e9
     traffic = None
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_kernel_rmat_s20_traffic.json")))
-        if prof.get("scale") == a.scale:
-            traffic = prof.get("dram_bytes_per_launch")
+        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_kernel_rmat_traffic.json")))
+        for rec in prof["records"]:
+            if (rec["scale"] == a.scale and abs(rec["alpha"] - a.alpha) < 1e-6
+                    and rec["bucket"] == a.bucket):
+                traffic = rec["dram_bytes_per_launch"]
     except Exception:
         pass
 

@@ -135,7 +135,7 @@ extern "C" reset_status reset_clique4_count(const reset_table* t, const int32_t*
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
   int32_t* d_mx = nullptr;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_mx), sizeof(int32_t), st));
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_mx), sizeof(int32_t), st));
   cudaError_t e = cudaMemsetAsync(d_mx, 0, sizeof(int32_t), st);
   if (e == cudaSuccess) {
     note_launch();
@@ -157,8 +157,8 @@ extern "C" reset_status reset_clique4_count(const reset_table* t, const int32_t*
   const int64_t warps = grid * kCqWarps;
   int32_t* d_scr = nullptr;
   unsigned long long* d_cur = nullptr;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_scr), sizeof(int32_t) * warps * cap, st));
-  e = cudaMallocAsync(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_scr), sizeof(int32_t) * warps * cap, st));
+  e = scratch_malloc(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_cur, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) {
     note_launch();

@@ -132,6 +132,9 @@ int sm_count();
 reset_tuning tuning();
 // The library-owned table memory pool of the current device.
 reset_status table_pool(cudaMemPool_t* out);
+// Stream-ordered scratch from the same pool (it keeps freed pages mapped,
+// unlike the device's default pool, which unmaps them at every sync).
+cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t st);
 // Vertex-staged triangle counting (tc_staged.cu); *count must be zeroed.
 reset_status tc_staged(const reset_table* t, const int4* desc,
                        const int32_t* d_cols, int64_t m,

@@ -594,7 +594,7 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
     rows = owned_rows;
   }
   unsigned long long* cursor = nullptr;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&cursor), sizeof(*cursor), st));
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&cursor), sizeof(*cursor), st));
   cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(*cursor), st);
   const reset_tuning tun = tuning();
   const int wpm = tun.warp_pair_min;
@@ -714,7 +714,7 @@ reset_status reset_intersect_count(const int32_t* d_a, int64_t na,
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int64_t), st));
   if (na == 0 || nb == 0) return RESET_OK;
   int32_t* d_offb = nullptr;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_offb), 2 * sizeof(int32_t), st));
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_offb), 2 * sizeof(int32_t), st));
   const int32_t h_offb[2] = {0, (int32_t)nb};
   RST_CUDA(cudaMemcpyAsync(d_offb, h_offb, sizeof(h_offb), cudaMemcpyHostToDevice, st));
   reset_table* t = nullptr;
@@ -774,8 +774,8 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
       return rs;                                                            \
     }                                                                       \
   } while (0)
-  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_sl), sizeof(int64_t) * (nq + 1), st));
-  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_tot), sizeof(int64_t) * 2, st));
+  IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_sl), sizeof(int64_t) * (nq + 1), st));
+  IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_tot), sizeof(int64_t) * 2, st));
   note_launch(); ir_plan_kernel<<<(int)clamp_grid((nq + 255) / 256, sm_count() * 8), 256, 0, st>>>(
       ds.desc, t->n, d_query, d_qoff, nq, d_sl, t->d_status);
   IR_CUDA(cudaGetLastError());
@@ -783,16 +783,16 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   IR_CUDA(cudaMemcpyAsync(d_tot + 1, d_sl + (nq - 1), sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
   size_t tb = 0;
   IR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_sl, d_sl, nq, st));
-  IR_CUDA(cudaMallocAsync(&d_tmp, tb, st));
+  IR_CUDA(scratch_malloc(&d_tmp, tb, st));
   IR_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tb, d_sl, d_sl, nq, st));
   note_launch(); ir_total_kernel<<<1, 1, 0, st>>>(d_tot + 1, d_sl, nq, d_tot);
   IR_CUDA(cudaGetLastError());
   int64_t total = 0;
   IR_CUDA(cudaMemcpyAsync(&total, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   IR_CUDA(cudaStreamSynchronize(st));
-  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_slc), sizeof(int32_t) * (total > 0 ? total : 1), st));
-  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_pos), sizeof(int64_t) * (total + 1), st));
-  IR_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_stage),
+  IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_slc), sizeof(int32_t) * (total > 0 ? total : 1), st));
+  IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_pos), sizeof(int64_t) * (total + 1), st));
+  IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_stage),
                           sizeof(int32_t) * (size_t)(total > 0 ? total : 1) * kIrSlice, st));
   rs = t->hier ? ir_run<true>(t, ds.desc, d_docs, d_query, d_qoff, nq, d_sl, total, d_res_off,
                               d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st)

@@ -198,7 +198,8 @@ struct Req {
   int64_t dev_bytes = 0;
   int64_t aux = 0;  // IR: df(first term); TC: number of (v, w) pairs; RAW: len
   reset_status status = RESET_OK;
-  BlockP docs_block;               // IR: survivors live in this pinned block
+  BlockP docs_block;               // IR: survivors live in this pinned block, or
+  std::vector<int32_t> docs_copy;  // in this copy when no block was free
   const int32_t* docs = nullptr;
   std::vector<int64_t> values;
   std::vector<uint8_t> flags;
@@ -257,14 +258,15 @@ struct Batch {
   int64_t reserved = 0;
   int64_t t_launch = 0;
   int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
-  BlockP res;     // pinned block receiving the IR survivors (phase 1)
+  BlockP res;     // pinned block receiving the IR survivors (phase 1), or
+  const int32_t* res_ptr = nullptr;  // the slot's own buffer (then copied out)
   reset_status status = RESET_OK;
 };
 
 struct Slot {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
-  Pinned in, out;
+  Pinned in, out, res;
   void* arena = nullptr;  // device buffer reused by this slot's batches
   size_t arena_cap = 0;
   std::unique_ptr<Batch> batch;  // set while in flight
@@ -680,8 +682,16 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
         const int32_t c = reinterpret_cast<const int32_t*>(at(g.out[0]))[r->item0];
         const int64_t o = reinterpret_cast<const int64_t*>(at(g.out[1]))[r->item0];
         r->count = c;
-        r->docs_block = c > 0 ? bt.res : nullptr;
-        r->docs = c > 0 ? static_cast<const int32_t*>(bt.res->p) + g.dense_host + o : nullptr;
+        const int32_t* src = bt.res_ptr + g.dense_host + o;
+        if (c == 0) {
+          r->docs = nullptr;
+        } else if (bt.res) {  // hand out the pinned block itself
+          r->docs_block = bt.res;
+          r->docs = src;
+        } else {              // the slot's buffer is reused: copy
+          r->docs_copy.assign(src, src + c);
+          r->docs = r->docs_copy.data();
+        }
         break;
       }
       case RESET_REQ_PAIRS: {
@@ -737,13 +747,15 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
 // known on the host) into the slot's pinned result buffer.  Returns true if
 // copies were enqueued (the batch completes at the next event).
 // A free pinned block of at least `bytes` from the pool (under the server
-// lock), or a new one.
+// lock), a new one while the pool holds fewer than two per stream, else
+// nullptr (the batch then lands in the slot's buffer and is copied out).
 BlockP take_block(reset_server* s, size_t bytes) {
   std::lock_guard<std::mutex> lk(s->mu);
   BlockP best;
   for (auto& b : s->blocks)
     if (b.use_count() == 1 && b->cap >= bytes && (!best || b->cap < best->cap)) best = b;
   if (best) return best;
+  if (s->blocks.size() >= 2 * s->slots.size()) return nullptr;
   auto b = std::make_shared<PinnedBlock>();
   const size_t cap = std::max(bytes, (size_t)(1u << 20));
   if (cudaHostAlloc(&b->p, cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
@@ -763,14 +775,19 @@ bool enqueue_results(reset_server* s, Slot& sl, Batch& bt) {
   }
   if (total == 0) return false;
   bt.res = take_block(s, 4 * total);
-  if (!bt.res) {
-    bt.status = cuda_fail(cudaErrorMemoryAllocation, "pinned result buffer", __FILE__, __LINE__);
-    return false;
+  if (bt.res) {
+    bt.res_ptr = static_cast<const int32_t*>(bt.res->p);
+  } else {
+    if (sl.res.ensure(4 * total) != cudaSuccess) {
+      bt.status = cuda_fail(cudaErrorMemoryAllocation, "pinned result buffer", __FILE__, __LINE__);
+      return false;
+    }
+    bt.res_ptr = static_cast<const int32_t*>(sl.res.p);
   }
   const char* dp = static_cast<const char*>(bt.d_buf);
   for (auto& g : bt.groups) {
     if (g.kind != RESET_REQ_IR || g.dense_n == 0) continue;
-    cudaError_t e = cudaMemcpyAsync(static_cast<int32_t*>(bt.res->p) + g.dense_host,
+    cudaError_t e = cudaMemcpyAsync(const_cast<int32_t*>(bt.res_ptr) + g.dense_host,
                                     dp + g.sc[2], 4 * (size_t)g.dense_n,
                                     cudaMemcpyDeviceToHost, sl.st);
     if (e != cudaSuccess) {
@@ -1079,6 +1096,7 @@ reset_status reset_server_destroy(reset_server* s) {
     if (sl.arena) cudaFree(sl.arena);
     sl.in.release();
     sl.out.release();
+    sl.res.release();
   }
   s->reqs.clear();
   s->blocks.clear();

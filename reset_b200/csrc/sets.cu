@@ -286,7 +286,7 @@ struct Temps {
   }
   template <class T>
   cudaError_t get(T** p, size_t bytes) {
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes ? bytes : 16, st);
+    cudaError_t e = scratch_malloc(reinterpret_cast<void**>(p), bytes ? bytes : 16, st);
     if (e == cudaSuccess) ptrs.push_back(*p);
     return e;
   }

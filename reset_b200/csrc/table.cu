@@ -494,7 +494,7 @@ int grid_for(int64_t items, int threads, int per_sm = 8) {
 reset_status make_chunk_rows(const int32_t* d_off, int32_t n, int64_t m,
                              int32_t** d_rows_out, cudaStream_t st) {
   int64_t nc = (m + 31) / 32;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d_rows_out),
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(d_rows_out),
                            sizeof(int32_t) * (nc > 0 ? nc : 1), st));
   RST_CUDA(cudaMemsetAsync(*d_rows_out, 0, sizeof(int32_t) * (nc > 0 ? nc : 1), st));
   note_launch(); layout_kernel<<<grid_for(n, 256), 256, 0, st>>>(
@@ -520,7 +520,7 @@ __global__ void redesc_kernel(const int32_t* __restrict__ off,
 
 reset_status make_desc(const reset_table* t, const int32_t* d_off,
                        int4** d_desc_out, cudaStream_t st) {
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d_desc_out),
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(d_desc_out),
                            sizeof(int4) * (t->n > 0 ? t->n : 1), st));
   note_launch(); redesc_kernel<<<grid_for(t->n, 256), 256, 0, st>>>(d_off, t->d_desc, t->n,
                                                      *d_desc_out);
@@ -557,6 +557,12 @@ reset_status table_pool(cudaMemPool_t* out) {
   }
   *out = g_pool[dev];
   return RESET_OK;
+}
+
+cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool;
+  if (table_pool(&pool) != RESET_OK) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
 
 void release_pools() {

@@ -316,8 +316,8 @@ reset_status tc_staged(const reset_table* t, const int4* desc,
   const int cap = (int)(mm / 128 + 64);
   int2* units = nullptr;
   int32_t* ctr = nullptr;
-  RST_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&units), sizeof(int2) * cap, st));
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ctr), sizeof(int32_t) * 4, st);
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&units), sizeof(int2) * cap, st));
+  cudaError_t e = scratch_malloc(reinterpret_cast<void**>(&ctr), sizeof(int32_t) * 4, st);
   if (e != cudaSuccess) {
     cudaFreeAsync(units, st);
     return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
