@@ -4,9 +4,9 @@ Runs the reference's own kernels (triangle-count/, set-similarity-search/,
 information-retrieval/, set_size/ compiled unchanged for sm_100a into
 oracle/_ref/ by `make -C oracle ref`) on small seeded inputs written in the
 reference's .bin formats, and packs inputs + reference outputs into
-compressed .npz files.  Needs a GPU; run on the GPU box:
+compressed .npz files.  Needs a GPU:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out /tmp/golden
 
 and copy the .npz files into tests/golden/.  Inputs come from the oracle's
 seeded generators, so they can be re-created anywhere.
