@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kIrSlice = 2048;  // candidates per IR work item
+constexpr int kIrSlice = 512;  // candidates per IR work item
 
 // Row of edge e (warp-collective).  u0 is the row of the chunk's first edge;
 // row(e) = u0 + #{j : off[u0+1+j] <= e}, searched 32 rows at a time.
