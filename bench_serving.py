@@ -437,15 +437,82 @@ def ir_serve_ours(a, rank, world, local):
                 "h2d_bytes_per_step": int(4 * qterms * a.requests + 20 * a.requests),
                 "d2h_bytes_per_step": int(4 * res_ints * a.requests + 4 * a.requests),
                 "note": "serving is end to end by construction: host query arrays in, "
-                        "host result lists out, through reset_server_*"},
+                        "host result lists out, through reset_server_*; d2h is an upper "
+                        "bound (first-term lengths; only survivors are copied)"},
         "roofline": None,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if rank == 0:
+        # exact total over all queries from one plain reset_ir call, for the
+        # native client's check
+        qd = torch.from_numpy(np.concatenate(reqs)).cuda()
+        qo = torch.from_numpy(np.r_[0, np.cumsum([x.size for x in reqs])].astype(np.int32)).cuda()
+        _, _, cnt = api.ir(t, toff, docs, qd, qo)
+        exact = int(cnt.sum().item())
+        del qd, qo, cnt
+        nat = _ir_native(h_toff, h_docs, reqs, [])   # burst: capacity cross-check
+        if nat is not None:
+            for v in nat.values():
+                if "total_results" in v:
+                    assert v["total_results"] == exact, "native client totals differ"
+        line["native_client"] = {"driver": "reset_b200/bin/reset_serve_ir", "runs": nat,
+                                 "exact_total_results": exact,
+                                 "note": "same queries and index, C++ client (4000 queries "
+                                         "of warm-up, then all at once), table built by the "
+                                         "driver (alpha 0.2, bucket 5)"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = _ir_cpu(h_toff, h_docs, reqs, a.cpu_seconds)
     t.free()
     _finish(line, rank, world)
+
+
+def _ir_native(h_toff, h_docs, reqs, rates):
+    """The same queries through the native serving driver
+    (reset_b200/bin/reset_serve_ir, C++ client on reset_server_*), reading
+    the index and queries in the reference's IR folder format: a burst and
+    Poisson arrivals at `rates`.  Returns per-run throughput, p50/p99 and the
+    total result count."""
+    import re
+    import shutil
+    import subprocess
+    import tempfile
+    exe = os.path.join(B.ROOT, "reset_b200", "bin", "reset_serve_ir")
+    if not os.path.exists(exe):
+        return None
+    d = tempfile.mkdtemp(prefix="reset_ir_")
+
+    def arr(name, x):
+        with open(os.path.join(d, name), "wb") as f:
+            np.array([x.size], np.uint64).tofile(f)
+            np.ascontiguousarray(x, np.int32).tofile(f)
+
+    def scal(name, x):
+        np.array([x], np.int32).tofile(os.path.join(d, name))
+
+    try:
+        arr("inverted_index_offsets.bin", h_toff)
+        arr("inverted_index.bin", h_docs)
+        scal("inverted_index_num.bin", h_toff.size - 1)
+        arr("query.bin", np.concatenate(reqs))
+        arr("query_offsets.bin", np.r_[0, np.cumsum([x.size for x in reqs])])
+        scal("query_num.bin", len(reqs))
+        out = {}
+        runs = [("burst", [])] + [(f"poisson_{int(r)}_per_s", [f"--rate={r:.0f}"]) for r in rates]
+        for label, extra in runs:
+            p = subprocess.run([exe, d, "--warmup=4000"] + extra, capture_output=True,
+                               text=True, timeout=900)
+            if p.returncode != 0:
+                out[label] = {"error": (p.stdout + p.stderr)[-300:]}
+                continue
+            m = re.search(r"served: ([0-9.]+) queries/s, latency p50 ([0-9.]+) ms, "
+                          r"p99 ([0-9.]+) ms", p.stdout)
+            tot = re.search(r"Total result count: (\d+)", p.stdout)
+            out[label] = {"queries_per_s": float(m.group(1)), "p50_ms": float(m.group(2)),
+                          "p99_ms": float(m.group(3)), "total_results": int(tot.group(1))}
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def _ir_cpu(toff, docs, reqs, seconds):

@@ -1,11 +1,13 @@
-// reset_serve_ir <folder> [--streams=N] [--max-batch=N] [--rate=QPS] [--alpha=F] [--bucket=N]
+// reset_serve_ir <folder> [--streams=N] [--max-batch=N] [--rate=QPS] [--warmup=N]
+//                [--alpha=F] [--bucket=N]
 // Serves the queries of a reference information-retrieval folder
 // (information-retrieval/ir.cu:213-267 input files: inverted_index_offsets.bin,
 // inverted_index.bin, inverted_index_num.bin, query.bin, query_offsets.bin,
 // query_num.bin) through the served form: the table stays resident, the
 // queries arrive all at once (default) or as a Poisson stream at --rate,
-// batches run continuously.  Prints the reference's total line, then
-// throughput and latency percentiles.
+// batches run continuously.  --warmup=N first serves the first N queries
+// once, untimed (buffers and memory pools reach their working size).  Prints
+// the reference's total line, then throughput and latency percentiles.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -22,7 +24,7 @@ int main(int argc, char** argv) {
             argv[0]);
     return 1;
   }
-  int streams = 4, max_batch = 1024, bucket = 5;
+  int streams = 4, max_batch = 1024, bucket = 5, warmup = 0;
   double rate = 0.0;
   float alpha = 0.2f;
   for (int i = 2; i < argc; i++) {
@@ -30,6 +32,7 @@ int main(int argc, char** argv) {
     if (a.rfind("--streams=", 0) == 0) streams = std::stoi(a.substr(10));
     else if (a.rfind("--max-batch=", 0) == 0) max_batch = std::stoi(a.substr(12));
     else if (a.rfind("--rate=", 0) == 0) rate = std::stod(a.substr(7));
+    else if (a.rfind("--warmup=", 0) == 0) warmup = std::stoi(a.substr(9));
     else if (a.rfind("--alpha=", 0) == 0) alpha = std::stof(a.substr(8));
     else if (a.rfind("--bucket=", 0) == 0) bucket = std::stoi(a.substr(9));
     else {
@@ -61,6 +64,13 @@ int main(int argc, char** argv) {
     {
       reset::Server srv(streams, max_batch);
       int ix = srv.add_index(t, idx.get_device_offsets(), idx.get_device_elements());
+      {  // untimed warm-up over the first queries
+        const int nw = std::min(std::max(warmup, 0), nq);
+        std::vector<uint64_t> wt(nw);
+        for (int i = 0; i < nw; i++)
+          wt[i] = srv.submit(RESET_REQ_IR, ix, q.data() + qoff[i], qoff[i + 1] - qoff[i]);
+        for (int i = 0; i < nw; i++) reset::check(srv.wait(wt[i]).status);
+      }
       std::vector<uint64_t> tickets(nq);
       std::mt19937_64 rng(12345);
       std::exponential_distribution<double> gap(rate > 0 ? rate : 1.0);
