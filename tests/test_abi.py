@@ -104,3 +104,34 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_new_entry_points_validate_on_the_host(libreset):
+    """Argument checks of the batched, served and generator entry points run
+    on the host before any CUDA call."""
+    from reset_b200 import _lib
+    out = ctypes.c_void_p()
+    cfg = _lib.ServerConfig()
+    libreset.reset_server_config_default(ctypes.byref(cfg))
+    assert cfg.streams == 4 and cfg.max_batch_requests == 1024
+    cfg.streams = 0
+    assert libreset.reset_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 3
+    cfg.streams, cfg.max_batch_requests = 4, 0
+    assert libreset.reset_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 3
+    # unknown batch option; NULL table
+    assert libreset.reset_batch_create_ex(ctypes.c_void_p(8), ctypes.c_void_p(8), 10, 7, 10,
+                                          1 << 5, ctypes.byref(out), None) == 3
+    assert libreset.reset_batch_create_ex(None, None, 10, 7, 10, 0, ctypes.byref(out),
+                                          None) == 3
+    po, pt, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int64()
+    assert libreset.reset_gen_token_sets(0, 10, 1.2, 8, 64, 0.0, 0.8, 1, ctypes.byref(po),
+                                         ctypes.byref(pt), ctypes.byref(m), None) == 3
+    assert libreset.reset_gen_token_sets(10, 10, 1.2, 8, 64, 1.5, 0.8, 1, ctypes.byref(po),
+                                         ctypes.byref(pt), ctypes.byref(m), None) == 3
+    assert libreset.reset_gen_inverted_index(0, 10, 1.1, 5, 1, ctypes.byref(po),
+                                             ctypes.byref(pt), ctypes.byref(m), None) == 3
+    assert libreset.reset_server_wait(None, 1, 0, None) == 3
+    t = _lib.Tuning()
+    libreset.reset_get_tuning(ctypes.byref(t))
+    bad = _lib.Tuning(t.probe_rounds, t.warp_pair_min, 7)
+    assert libreset.reset_set_tuning(ctypes.byref(bad)) == 3
