@@ -44,7 +44,24 @@ sys.path.insert(0, ROOT)
 
 METRIC = "TC edges/sec (R-MAT scale 24, table build + hash-probe count)"
 UNIT = "edges/s"
-SEED = 0x5EED0024
+
+
+def rmat_seed(scale: int) -> int:
+    """0x5EED00SS, SS = the scale's decimal digits (scale 24 -> 0x5EED0024)."""
+    return int(f"0x5EED00{scale:02d}", 16)
+
+
+def oracle_count(scale: int, edge_factor: int):
+    """The CPU oracle's exact triangle count of the seeded graph of this
+    scale (tests/golden/tc_counts.json), or None if it was not computed."""
+    try:
+        rec = json.load(open(os.path.join(ROOT, "tests", "golden", "tc_counts.json")))
+        if rec.get("edge_factor") != edge_factor:
+            return None
+        c = rec["counts"].get(str(scale))
+        return c if c and int(c["seed"], 16) == rmat_seed(scale) else None
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def parse():
@@ -62,8 +79,9 @@ def parse():
     ap.add_argument("--warp-pair-min", type=int, default=0)
     ap.add_argument("--probe-variant", type=int, default=-1, choices=[-1, 0, 1],
                     help="-1 library default; 0 pipelined; 1 lean whole-warp pair loop")
-    ap.add_argument("--tc-method", type=int, default=0, choices=[0, 1, 2],
-                    help="0 default (edge-flattened), 1 edge-flattened, 2 vertex-staged")
+    ap.add_argument("--tc-method", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="0 default (owner-grouped), 1 edge-flattened, 2 vertex-staged, "
+                         "3 owner-grouped (probed tables staged in shared memory)")
     ap.add_argument("--alpha", type=float, default=0.2,
                     help="TC table load factor (with --no-autotune)")
     ap.add_argument("--bucket", type=int, default=5,
@@ -227,7 +245,7 @@ def run_ours(a, rank, world, local):
                        warp_pair_min=a.warp_pair_min or None,
                        probe_variant=a.probe_variant if a.probe_variant >= 0 else None)
 
-    off, cols = api.gen_rmat(a.scale, a.edge_factor, SEED)
+    off, cols = api.gen_rmat(a.scale, a.edge_factor, rmat_seed(a.scale))
     n, m = off.numel() - 1, cols.numel()
     deg = (off[1:] - off[:-1])
     src = torch.repeat_interleave(torch.arange(n, device="cuda", dtype=torch.int64), deg.long())
@@ -259,9 +277,13 @@ def run_ours(a, rank, world, local):
 
         deg = (off[1:] - off[:-1]).cpu().numpy()
         samp = deg[np.random.default_rng(1).integers(0, deg.size, min(deg.size, 200_000))]
-        hp = autotune.solve("tc", samp, measure=measure, measure_top=3, rounds=(4, 8),
-                            warp_pair_mins=(32, 64, 128), cache=None,
-                            always=((0.2, 5), (0.25, 1), (0.4, 2)))
+        # the probe-round and warp-pair knobs steer the edge-flattened kernel
+        # only; the owner-grouped count is tuned over (alpha, b) alone
+        edge = a.tc_method == 1
+        hp = autotune.solve("tc", samp, measure=measure, measure_top=3,
+                            rounds=(4, 8) if edge else (),
+                            warp_pair_mins=(32, 64, 128) if edge else (), cache=None,
+                            always=((0.2, 5), (0.25, 1), (0.4, 2), (0.5, 1), (0.5, 2)))
         api.set_tuning(probe_rounds=hp.probe_rounds, warp_pair_min=hp.warp_pair_min,
                        probe_variant=1)
         a.alpha, a.bucket = hp.alpha, hp.b
@@ -326,6 +348,15 @@ def run_ours(a, rank, world, local):
     torch.cuda.synchronize()
     expect = int(counts[-1].item())
     counts.clear()
+    # parity, outside the timed region: the exact count the CPU oracle
+    # computed on the same seeded graph
+    pinned = oracle_count(a.scale, a.edge_factor)
+    if pinned is not None:
+        assert pinned["vertices"] == n and pinned["oriented_edges"] == m, "graph differs"
+        assert expect == pinned["triangles"], \
+            f"triangle count {expect} != oracle {pinned['triangles']}"
+    parity = ("equals the CPU oracle's count of the same graph (tests/golden/tc_counts.json)"
+              if pinned is not None else "unpinned at this scale (no oracle count on file)")
 
     l0 = L.reset_kernel_launches()
     barrier()
@@ -391,9 +422,11 @@ def run_ours(a, rank, world, local):
         "dtype": "int32", "data": "synthetic (seeded R-MAT generated on device)",
         "config": {"workload": f"tc_rmat_s{a.scale}_ef{a.edge_factor}",
                    "scale": a.scale, "edge_factor": a.edge_factor, "vertices": n,
-                   "oriented_edges": m, "triangles": expect, "probes": sum_s,
+                   "oriented_edges": m, "triangles": expect, "parity": parity,
+                   "probes": sum_s,
                    "alpha": a.alpha, "bucket": a.bucket, "hash": "hierarchical",
-                   "tc_method": ["edge-flattened", "edge-flattened", "vertex-staged"][a.tc_method],
+                   "tc_method": ["owner-grouped", "edge-flattened", "vertex-staged",
+                                 "owner-grouped"][a.tc_method],
                    "tuning": api.get_tuning(), "autotuned": tuned,
                    "vertex_ids": "relabeled by a seeded bijection (Graph500 convention)",
                    "parallelism": f"replicas x{world}",
@@ -404,7 +437,10 @@ def run_ours(a, rank, world, local):
         "probe_only": {"value": weak_value(m, world, probe_avg), "unit": UNIT,
                        "ms_per_launch": probe_avg},
         "roofline": {"bound": "hbm",
-                     "kernel": "tc_staged_kernel" if a.tc_method == 2 else "tc_kernel",
+                     "kernel": ["tc_owner_kernel + its grouping passes", "tc_kernel",
+                                "tc_staged_kernel",
+                                "tc_owner_kernel + its grouping passes"][a.tc_method],
+                     "timed": "the whole reset_tc_count_ex call (CUDA events on its stream)",
                      "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": traffic,
@@ -435,7 +471,7 @@ def run_reference(a, rank, world):
     import oracle
     thr = host_threads()
     t0 = time.perf_counter()
-    off, cols = oracle.rmat_graph(a.scale, a.edge_factor, SEED, oriented=True)
+    off, cols = oracle.rmat_graph(a.scale, a.edge_factor, rmat_seed(a.scale), oriented=True)
     gen_s = time.perf_counter() - t0
     rates = []
     info = None

@@ -116,8 +116,10 @@ reset_status reset_table_free_async(reset_table *t, reset_stream_t stream);
 reset_status reset_release_cached_memory(void);
 
 /* Synchronise `stream` and report device-side errors raised by kernels that
- * used this table since the last call (RESET_ERR_PROBE_LIMIT,
- * RESET_ERR_TABLE_FULL), then clear them. */
+ * used this table since the last call (RESET_ERR_TABLE_FULL,
+ * RESET_ERR_PROBE_LIMIT, RESET_ERR_ARG for a row, pair or query id outside
+ * [0, n), RESET_ERR_TIMEOUT for a bounded wait that gave up), then clear
+ * them. */
 reset_status reset_table_check(reset_table *t, reset_stream_t stream);
 
 /* Rows of the table's CSR read back in bucket order (slot-major within each
@@ -159,10 +161,13 @@ reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
  * Its scratch (four work counters and up to 2^20 work units, 8 MiB) is one
  * fixed device array inside libreset.so, present on every GPU that loads the
  * library until the process exits.  Limits: at most 134,209,536 edges (m and
- * the table's own edge count), and d_off must be NULL or the offsets the
- * table was built from; otherwise RESET_ERR_ARG.  The first call on a device
- * looks up the array's device address (once per device), so make that first
- * call before any stream capture.  All calls share the array and the array
+ * the table's own edge count), d_off must be NULL or the offsets the table
+ * was built from, and m must equal the table's edge count (d_cols is the
+ * build CSR's column array, or a row-wise permutation of it such as the
+ * hash-ordered rows); otherwise RESET_ERR_ARG.  The first call on a device
+ * looks up the array's device address (once per device, kept for the life
+ * of the device's primary context: do not call it again after a
+ * cudaDeviceReset), so make that first call before any stream capture.  All calls share the array and the array
  * keeps the last call's contents (the counters are cleared at every call):
  * calls that overlap on the GPU -- on different streams, or from different
  * threads -- race on it and must be serialised by the caller. */

@@ -60,13 +60,15 @@ inline void check(cudaError_t e, const char* what) {
 }
 
 inline void parse_params(int argc, char** argv, int first, float* alpha,
-                         int* bucket) {
+                         int* bucket, bool* no_dump = nullptr) {
   for (int i = first; i < argc; i++) {
     std::string a = argv[i];
     if (a.rfind("--alpha=", 0) == 0)
       *alpha = std::stof(a.substr(8));
     else if (a.rfind("--bucket=", 0) == 0)
       *bucket = std::stoi(a.substr(9));
+    else if (a == "--no-dump" && no_dump)  // results on stdout only, no table files
+      *no_dump = true;
     else
       die("unknown argument " + a);
   }

@@ -74,7 +74,13 @@ inline RefTables ref_build_tables(const vector<int>& off,
   hio::check(cudaMemcpy(t.off64.data(), t.d_off64, sizeof(long long) * n, cudaMemcpyDeviceToHost), "d2h");
   t.bucket_num = t.off64[n - 1] + t.len[n - 1];
   t.off64[n] = t.bucket_num;
-  if ((long long)b * t.bucket_num >= (1LL << 31)) hio::die("bucket_num too large for the 32-bit slot index");
+  // the reference's kernels index slots as int `bucket + k * bucket_num`
+  // (bucket < max_len, k < b; TC.cu:18, hashtable.cu:65): refuse inputs
+  // where that overflows, before any kernel runs
+  const long long max_index = (long long)(b - 1) * t.bucket_num + t.max_len - 1;
+  printf("ref tables: bucket_num=%lld max_len=%d largest int slot index=%lld (limit %lld)\n",
+         t.bucket_num, t.max_len, max_index, (1LL << 31) - 1);
+  if (max_index >= (1LL << 31)) hio::die("bucket_num too large for the reference's 32-bit slot index");
   hio::check(cudaMemcpy(t.d_off64 + n, &t.bucket_num, sizeof(long long), cudaMemcpyHostToDevice), "h2d");
   size_t tbytes = sizeof(int) * (size_t)t.bucket_num * b;
   hio::check(cudaMalloc(&t.d_tn, tbytes), "malloc");

@@ -16,11 +16,12 @@ __global__ void dynamic_triangle_count(
     int max_length, int bucket_num, int bucket_size);
 
 int main(int argc, char** argv) {
-  if (argc < 3) hio::die("usage: ref_tc <in_dir> <out_dir> [--alpha=F] [--bucket=N]");
+  if (argc < 3) hio::die("usage: ref_tc <in_dir> <out_dir> [--alpha=F] [--bucket=N] [--no-dump]");
   std::string in = argv[1], out = argv[2];
   float alpha = 0.2f;
   int b = 5;
-  hio::parse_params(argc, argv, 3, &alpha, &b);
+  bool no_dump = false;
+  hio::parse_params(argc, argv, 3, &alpha, &b, &no_dump);
   vector<int> off = hio::read_arr<int>(in + "/csr_offsets_tri.bin");
   vector<int> cols = hio::read_arr<int>(in + "/csr_cols_tri.bin");
   int n = hio::read_scalar(in + "/num_nodes_tri.bin");
@@ -58,9 +59,11 @@ int main(int argc, char** argv) {
     hio::check(cudaMemcpy(&counts[opt], d_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost), "d2h");
   }
   long long meta[4] = {t.max_len, t.bucket_num, (long long)counts[0], (long long)counts[1]};
-  hio::write_arr(out + "/meta.i64.bin", meta, 4);
-  ref_dump_tables(t, out);
-  hio::write_vec(out + "/cols_hier_sorted.bin", cols_h);
+  if (!no_dump) {
+    hio::write_arr(out + "/meta.i64.bin", meta, 4);
+    ref_dump_tables(t, out);
+    hio::write_vec(out + "/cols_hier_sorted.bin", cols_h);
+  }
   printf("ref_tc n=%d m=%d max_len=%d bucket_num=%lld normal=%llu (%.3f ms) hier=%llu (%.3f ms)\n", n, m, t.max_len, t.bucket_num, counts[0], ms[0], counts[1], ms[1]);
   return 0;
 }

@@ -9,7 +9,12 @@ to the device generator), is written in the reference's TC input format
 kernel time of dynamic_triangle_count (TC.cu:128-190, launch shape of
 TC.cu:268-275) in both hash modes, timed with CUDA events.
 
-    python oracle/ref_bench.py --scale 22 [--workdir DIR]
+    python oracle/ref_bench.py --scale 24 [--alpha 0.2 --bucket 5] [--workdir DIR]
+
+Before any kernel runs, the harness refuses graphs whose tables would
+overflow the reference's 32-bit slot index (bucket + k * bucket_num); the
+printed line gives bucket_num and the largest index.  Counts are compared
+with the oracle's count of the same graph (tests/golden/tc_counts.json).
 """
 import argparse
 import os
@@ -39,11 +44,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--edge-factor", type=int, default=16)
-    ap.add_argument("--seed", type=lambda s: int(s, 0), default=0x5EED0024)
+    ap.add_argument("--seed", type=lambda s: int(s, 0), default=None,
+                    help="default 0x5EED00SS, SS = the scale's decimal digits")
+    ap.add_argument("--alpha", type=float, default=0.2)
+    ap.add_argument("--bucket", type=int, default=5)
     ap.add_argument("--workdir", default=None)
     a = ap.parse_args()
     import oracle
-    seed = a.seed
+    seed = a.seed if a.seed is not None else int(f"0x5EED00{a.scale:02d}", 16)
     exe = os.path.join(HERE, "_ref", "ref_tc")
     if not os.path.exists(exe):
         sys.exit("oracle/_ref/ref_tc is missing (build it with `make -C oracle ref`)")
@@ -61,11 +69,26 @@ def main():
         write_int(os.path.join(ind, "num_edges_tri.bin"), cols.size)
         print(f"graph: scale {a.scale} seed {seed:#x} n={off.size - 1} m={cols.size} "
               f"(CPU generator {gen:.1f} s)", flush=True)
-        r = subprocess.run([exe, ind, outd], capture_output=True, text=True)
+        r = subprocess.run([exe, ind, outd, f"--alpha={a.alpha}", f"--bucket={a.bucket}",
+                            "--no-dump"], capture_output=True, text=True)
         print(r.stdout.strip())
         if r.returncode != 0:
             print(r.stderr.strip(), file=sys.stderr)
-        return r.returncode
+            return r.returncode
+        import json
+        try:
+            rec = json.load(open(os.path.join(os.path.dirname(HERE), "tests", "golden",
+                                              "tc_counts.json")))["counts"].get(str(a.scale))
+        except OSError:
+            rec = None
+        if rec and int(rec["seed"], 16) == seed:
+            import re
+            got = [int(x) for x in re.findall(r"(?:normal|hier)=(\d+)", r.stdout)]
+            ok = bool(got) and all(g == rec["triangles"] for g in got)
+            print(f"oracle count {rec['triangles']}: reference counts {got} "
+                  f"{'equal' if ok else 'DIFFER'}")
+            return 0 if ok else 1
+        return 0
     finally:
         shutil.rmtree(work, ignore_errors=True)
 

@@ -138,7 +138,10 @@ class Table:
             pass
 
 
-TC_DEFAULT, TC_EDGE, TC_STAGED = 0, 1, 2
+# reset_tc_count_ex methods: 0 default (owner-grouped when the columns are
+# 16-byte aligned, else edge-flattened), 1 edge-flattened, 2 vertex-staged,
+# 3 owner-grouped (probed tables staged in shared memory)
+TC_DEFAULT, TC_EDGE, TC_STAGED, TC_OWNER = 0, 1, 2, 3
 
 
 def tc_count_async(t: Table, off: torch.Tensor, cols: torch.Tensor,

@@ -35,6 +35,8 @@ reset_status arg_fail(const char* what);
 enum : int32_t {
   kErrTableFull = 1,
   kErrProbeLimit = 2,
+  kErrBadId = 4,       // a row or pair id outside [0, n)
+  kErrStageTimeout = 8,  // a bounded wait for a bulk copy into shared memory gave up
 };
 
 constexpr uint32_t kFull = 0xffffffffu;
@@ -139,6 +141,12 @@ cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t st);
 reset_status tc_staged(const reset_table* t, const int4* desc,
                        const int32_t* d_cols, int64_t m,
                        unsigned long long* count, cudaStream_t st);
+// Owner-grouped triangle counting (tc_owner.cu): tables staged in shared
+// memory, probers' rows streamed with 16-byte loads (d_cols 16-byte
+// aligned); *count must be zeroed.
+reset_status tc_owner(const reset_table* t, const int4* desc, const int32_t* d_off,
+                      const int32_t* d_cols, const int32_t* chunk_rows, int64_t m,
+                      unsigned long long* count, cudaStream_t st);
 // Counts launches of libreset's own kernels (reset_kernel_launches()).
 void note_launch(int k = 1);
 }  // namespace rst

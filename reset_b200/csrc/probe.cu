@@ -30,29 +30,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kIrSlice = 512;  // candidates per IR work item
 
-// Row of edge e (warp-collective).  u0 is the row of the chunk's first edge;
-// row(e) = u0 + #{j : off[u0+1+j] <= e}, searched 32 rows at a time.
-__device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
-                                           int n, int u0, int e) {
-  const int lane = threadIdx.x & 31;
-  int row = -1;
-  for (int ub = u0;; ub += 32) {
-    const int idx = ub + 1 + lane;
-    const int q = idx <= n ? __ldg(off + idx) : INT_MAX;
-    int c = 0;
-#pragma unroll
-    for (int step = 16; step >= 1; step >>= 1) {
-      int qq = __shfl_sync(kFull, q, c + step - 1);
-      if (qq <= e) c += step;
-    }
-    const int q31 = __shfl_sync(kFull, q, 31);
-    if (c == 31 && q31 <= e) c = 32;
-    if (row < 0 && c < 32) row = ub + c;
-    if (__all_sync(kFull, row >= 0)) break;
-  }
-  return row;
-}
-
 // ----------------------------------------------------------------- TC ----
 
 template <bool HIER, int ROUNDS, bool LEAN>
@@ -579,7 +556,11 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   if (!t || !d_count) return arg_fail("NULL table or count");
   if (m < 0 || m > INT32_MAX) return arg_fail("m out of range");
   if (m > 0 && (!d_cols || !d_off)) return arg_fail("NULL offsets or cols");
-  if (method < 0 || method > 2) return arg_fail("method must be 0, 1 or 2");
+  if (method < 0 || method > 3) return arg_fail("method must be 0, 1, 2 or 3");
+  const bool cols16 = (reinterpret_cast<uintptr_t>(d_cols) & 15) == 0;
+  if (method == 3 && !cols16)
+    return arg_fail("method 3 needs a 16-byte aligned column array");
+  if (method == 0) method = cols16 ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
@@ -592,6 +573,11 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   if (d_off != t->build_off || m != t->m) {
     RST_CHECK(make_chunk_rows(d_off, t->n, m, &owned_rows, st));
     rows = owned_rows;
+  }
+  if (method == 3) {
+    reset_status s = tc_owner(t, ds.desc, d_off, d_cols, rows, m, cnt, st);
+    if (owned_rows) cudaFreeAsync(owned_rows, st);
+    return s;
   }
   unsigned long long* cursor = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&cursor), sizeof(*cursor), st));

@@ -1,11 +1,34 @@
 // Device helpers shared by the probe kernels.
 #pragma once
 
+#include <climits>
+
 #include "common.cuh"
 
 namespace rst {
 
-enum : int32_t { kErrBadId = 4 };
+// Row of edge e (warp-collective).  u0 is the row of the chunk's first edge;
+// row(e) = u0 + #{j : off[u0+1+j] <= e}, searched 32 rows at a time.
+__device__ __forceinline__ int row_of_edge(const int32_t* __restrict__ off,
+                                           int n, int u0, int e) {
+  const int lane = threadIdx.x & 31;
+  int row = -1;
+  for (int ub = u0;; ub += 32) {
+    const int idx = ub + 1 + lane;
+    const int q = idx <= n ? __ldg(off + idx) : INT_MAX;
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      int qq = __shfl_sync(kFull, q, c + step - 1);
+      if (qq <= e) c += step;
+    }
+    const int q31 = __shfl_sync(kFull, q, 31);
+    if (c == 31 && q31 <= e) c = 32;
+    if (row < 0 && c < 32) row = ub + c;
+    if (__all_sync(kFull, row >= 0)) break;
+  }
+  return row;
+}
 
 // search_in_hashtable (triangle-count/TC.cu:11-31): walk the slots of the
 // home bucket, then the next bucket (mod len); equal slot = hit, -1 = miss.

@@ -809,6 +809,14 @@ reset_status reset_table_check(reset_table* t, reset_stream_t stream) {
     set_error("a probe walked a whole table without finding an empty slot");
     return RESET_ERR_PROBE_LIMIT;
   }
+  if (bits & kErrBadId) {
+    set_error("invalid argument: a row, pair or query id was outside [0, n)");
+    return RESET_ERR_ARG;
+  }
+  if (bits & kErrStageTimeout) {
+    set_error("a bounded wait for a shared-memory bulk copy gave up");
+    return RESET_ERR_TIMEOUT;
+  }
   return RESET_OK;
 }
 

@@ -1,4 +1,5 @@
-// Vertex-staged triangle counting (the default path of reset_tc_count).
+// Vertex-staged triangle counting (method 2 of reset_tc_count_ex; used by
+// reset_tc_count_noalloc).
 //
 // Same count as dynamic_triangle_count (triangle-count/TC.cu:128-190): for
 // every oriented edge (u, v) the smaller row is probed against the larger
@@ -382,7 +383,9 @@ std::mutex g_noalloc_mu;
 int2* g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device; looked up once
-// per device (the host-side symbol is not a device address).
+// per device (the host-side symbol is not a device address).  The cached
+// address holds for the life of the device's primary context: a process that
+// resets the device (cudaDeviceReset) must not call this entry point again.
 reset_status noalloc_scratch(int2** out) {
   int dev = 0;
   RST_CUDA(cudaGetDevice(&dev));
@@ -411,6 +414,10 @@ extern "C" reset_status reset_tc_count_noalloc(const reset_table* t,
   if (m > 0 && !d_cols) return arg_fail("NULL cols");
   if (d_off && d_off != t->build_off)
     return arg_fail("reset_tc_count_noalloc needs the offsets the table was built from");
+  // the kernel walks rows through the table's build-time descriptors, so the
+  // column array must be the one of the build CSR (same length)
+  if (m != t->m)
+    return arg_fail("reset_tc_count_noalloc needs m equal to the table's edge count");
   if (m > kNoAllocMaxEdges || t->m > kNoAllocMaxEdges) {
     set_error("invalid argument: reset_tc_count_noalloc takes at most %lld edges "
               "(its fixed scratch holds %d work units)",

@@ -300,7 +300,7 @@ def test_tc_methods_on_ragged_rows(R, cuda, oracle_mod, hier):
     want = oracle_mod.tc_hash(ot)
     doff, dcols = dev(off, cuda), dev(cols, cuda)
     t = R.Table(doff, dcols, hierarchical=hier, hash_order=True)
-    for method in (R.TC_EDGE, R.TC_STAGED):
+    for method in (R.TC_EDGE, R.TC_STAGED, R.TC_OWNER):
         assert R.tc_count(t, doff, dcols, method=method) == want
         assert R.tc_count(t, doff, t.hash_order, method=method) == oracle_mod.tc_hash(ot, ot.hash_order())
     t.check()
@@ -311,8 +311,54 @@ def test_tc_methods_agree_rmat(R, cuda, oracle_mod, scale):
     off, cols = R.gen_rmat(scale, 16, 0x5EED0100 + scale, oriented=True)
     want = oracle_mod.tc_merge(off.cpu().numpy(), cols.cpu().numpy())
     t = R.Table(off, cols, hash_order=True)
-    for method in (R.TC_EDGE, R.TC_STAGED):
+    for method in (R.TC_EDGE, R.TC_STAGED, R.TC_OWNER):
         assert R.tc_count(t, off, t.hash_order, method=method) == want
+
+
+def _fixture_counts():
+    import json
+    import os
+    p = os.path.join(os.path.dirname(__file__), "golden", "tc_counts.json")
+    return json.load(open(p))["counts"]
+
+
+@pytest.mark.parametrize("scale", [16, 18, 20, 22, 24])
+def test_tc_benchmark_graphs_match_oracle_counts(R, cuda, scale):
+    """The benchmark's graphs at full size (scale 24: 16.8M vertices, 260M
+    oriented edges): the device generator's graph, its tables (the
+    reference's alpha 0.2 / 5 slots, and 0.4 / 2) and every TC method give
+    the triangle count the CPU oracle computed on the same seeded graph
+    (tests/golden/tc_counts.json, made by make_tc_counts.py)."""
+    rec = _fixture_counts()[str(scale)]
+    off, cols = R.gen_rmat(scale, 16, int(rec["seed"], 16), oriented=True)
+    assert off.numel() - 1 == rec["vertices"] and cols.numel() == rec["oriented_edges"]
+    methods = (R.TC_OWNER, R.TC_EDGE) if scale >= 22 else (R.TC_OWNER, R.TC_EDGE, R.TC_STAGED)
+    for alpha, bucket in [(0.2, 5), (0.4, 2)]:
+        t = R.Table(off, cols, alpha=alpha, bucket=bucket, hierarchical=True, hash_order=True)
+        for method in methods:
+            assert R.tc_count(t, off, t.hash_order, method=method) == rec["triangles"], \
+                (alpha, bucket, method)
+        t.check()
+        t.free()
+
+
+def test_tc_owner_alignment_rules(R, cuda, oracle_mod):
+    """Method 3 streams rows with 16-byte loads: a column array that is not
+    16-byte aligned is refused by method 3 and counted by method 1 under the
+    default method."""
+    torch = cuda
+    off, cols = oracle_mod.rmat_graph(10, 16, 0x5EED0010, oriented=True)
+    want = oracle_mod.tc_merge(off, cols)
+    doff = dev(off, torch)
+    buf = torch.zeros(cols.size + 1, dtype=torch.int32, device="cuda")
+    buf[1:] = dev(cols, torch)
+    shifted = buf[1:]                      # 4-byte offset from a 256-byte aligned base
+    assert shifted.data_ptr() % 16 == 4
+    t = R.Table(doff, shifted, hierarchical=True)
+    assert R.tc_count(t, doff, shifted) == want
+    from reset_b200._lib import ResetError
+    with pytest.raises(ResetError):
+        R.tc_count(t, doff, shifted, method=R.TC_OWNER)
 
 
 # --------------------------------------------------------- tuning knobs --

@@ -74,3 +74,28 @@ def test_noalloc_rejects_what_it_cannot_hold(cuda, libreset):
     st = libreset.reset_tc_count_noalloc(t.handle, _ptr(off.clone()), _ptr(cols),
                                          cols.numel(), _ptr(out), s)
     assert st == 3
+    # a column count other than the table's: rows are walked through the
+    # build-time descriptors, so a shorter array would be read past its end
+    st = libreset.reset_tc_count_noalloc(t.handle, _ptr(off), _ptr(cols),
+                                         cols.numel() - 1, _ptr(out), s)
+    assert st == 3 and b"edge count" in libreset.reset_last_error_string()
+
+
+@pytest.mark.parametrize("name", ["tc_s10", "tc_s11_a05_b3"])
+def test_noalloc_equals_reference_golden_count(cuda, libreset, name):
+    """Against the triangle counts the reference's own kernel produced on the
+    same graphs (golden fixtures), both hashes, on the fixture's alpha and
+    bucket size."""
+    import os
+    torch = cuda
+    from reset_b200 import api
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    _, _, c_norm, c_hier = (int(x) for x in g["ref_meta"])
+    off = torch.from_numpy(g["off"]).cuda()
+    cols = torch.from_numpy(g["cols"]).cuda()
+    for hier, want in ((False, c_norm), (True, c_hier)):
+        t = api.Table(off, cols, alpha=float(g["alpha"]), bucket=int(g["bucket"]),
+                      hierarchical=hier)
+        for _ in range(2):
+            assert _noalloc(libreset, torch, t, off, cols) == want
+        t.check()
