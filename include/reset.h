@@ -280,6 +280,44 @@ reset_status reset_intersect_count(const int32_t *d_a, int64_t na,
                                    const reset_params *params,
                                    int64_t *d_count, reset_stream_t stream);
 
+/* ---- element-modulo sharding -------------------------------------------- */
+/* Shard `shard` of `shards` of a CSR: every row keeps, in order, its
+ * elements x with x % shards == shard (C remainder), the per-device input of
+ * the reference's multi-GPU programs (multi-GPU/tc-multi-GPU/main.cu:113-130,
+ * multi-GPU/sss-multi-GPU/main.cu:124-136).  d_off_out has n + 1 entries,
+ * d_cols_out room for m; *d_m_out (device, optional) receives the shard's
+ * element count.  No host synchronisation. */
+reset_status reset_csr_shard(const int32_t *d_off, const int32_t *d_cols,
+                             int32_t n, int64_t m, int32_t shards,
+                             int32_t shard, int32_t *d_off_out,
+                             int32_t *d_cols_out, int64_t *d_m_out,
+                             reset_stream_t stream);
+
+/* Partial triangle count of one shard, replacing partial_tc
+ * (multi-GPU/tc-multi-GPU/tc.cu:264): sum over the edges (u, v) of the
+ * full edge CSR of |K(u) ∩ K(v)|, where K is the shard CSR (d_key_off,
+ * d_key_cols, 16-byte aligned) that `t` was built on; the smaller shard row
+ * probes the larger one's table.  Summed over all shards (on one device or
+ * across devices) it equals reset_tc_count of the full graph (rows without
+ * repeated entries).  *d_count (device u64) is overwritten. */
+reset_status reset_tc_count_shard(const reset_table *t, const int32_t *d_key_off,
+                                  const int32_t *d_key_cols, int64_t m_keys,
+                                  const int32_t *d_edge_off,
+                                  const int32_t *d_edge_cols, int64_t m_edges,
+                                  uint64_t *d_count, reset_stream_t stream);
+
+/* Set-similarity decisions from intersection sizes summed over shards
+ * (multi-GPU/sss-multi-GPU/main.cu:144-151, with the exact integer rule):
+ * d_flags[p] = U > 0 && den * I >= num * U, I = d_inter[p],
+ * U = |A| + |B| - I with the full sets' sizes from d_off.  Pair ids outside
+ * [0, n) give flag 0 and set bit 4 (an out-of-range id) in *d_status_bits
+ * (optional). */
+reset_status reset_sss_decide(const int32_t *d_off, int32_t n,
+                              const int32_t *d_pair_a, const int32_t *d_pair_b,
+                              int64_t npairs, const int32_t *d_inter,
+                              int32_t num, int32_t den, uint8_t *d_flags,
+                              int32_t *d_status_bits, reset_stream_t stream);
+
 /* ---- synthetic inputs (stand-ins for the reference's datasets) -------- */
 
 /* Options of reset_gen_rmat. */
@@ -430,7 +468,12 @@ typedef struct reset_tuning {
   int32_t warp_pair_min; /* pairs with >= this many keys get a whole warp   */
   int32_t probe_variant; /* whole-warp pair loop: 0 = software-pipelined,
                             1 = lean (branch-free resolve, no prefetch)     */
-  int32_t reserved[5];
+  int32_t pair_method;   /* reset_sss / reset_sss_float: 0 = default
+                            (owner-grouped when the elements are 16-byte
+                            aligned), 1 = pair-flattened (with early exit
+                            when deciding only), 2 = owner-grouped (tables
+                            staged in shared memory)                         */
+  int32_t reserved[4];
 } reset_tuning;
 
 reset_status reset_get_tuning(reset_tuning *out);

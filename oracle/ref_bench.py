@@ -46,6 +46,8 @@ def main():
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--seed", type=lambda s: int(s, 0), default=None,
                     help="default 0x5EED00SS, SS = the scale's decimal digits")
+    ap.add_argument("--device-gen", action="store_true",
+                    help="generate the graph with the library's device generator")
     ap.add_argument("--alpha", type=float, default=0.2)
     ap.add_argument("--bucket", type=int, default=5)
     ap.add_argument("--workdir", default=None)
@@ -56,7 +58,17 @@ def main():
     if not os.path.exists(exe):
         sys.exit("oracle/_ref/ref_tc is missing (build it with `make -C oracle ref`)")
     t0 = time.perf_counter()
-    off, cols = oracle.rmat_graph(a.scale, a.edge_factor, seed, oriented=True)
+    if a.device_gen:
+        # the library's device generator: the same graph bit for bit (the
+        # GPU parity tests compare it with the oracle's), minutes faster
+        import torch
+        from reset_b200 import api
+        d_off, d_cols = api.gen_rmat(a.scale, a.edge_factor, seed, oriented=True)
+        off, cols = d_off.cpu().numpy(), d_cols.cpu().numpy()
+        del d_off, d_cols
+        torch.cuda.empty_cache()
+    else:
+        off, cols = oracle.rmat_graph(a.scale, a.edge_factor, seed, oriented=True)
     gen = time.perf_counter() - t0
     work = a.workdir or tempfile.mkdtemp(prefix="reset_ref_tc_")
     ind, outd = os.path.join(work, "in"), os.path.join(work, "out")

@@ -32,7 +32,8 @@ class Params(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("probe_rounds", C.c_int32), ("warp_pair_min", C.c_int32),
-                ("probe_variant", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("probe_variant", C.c_int32), ("pair_method", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class TableView(C.Structure):
@@ -99,6 +100,9 @@ SIGNATURES = {
     "reset_sss_float": (I32, [P, P, P, P, P, I64, C.c_float, P, P, P]),
     "reset_ir": (I32, [P, P, P, P, P, I32, P, P, P, P]),
     "reset_intersect_count": (I32, [P, I64, P, I64, C.POINTER(Params), P, P]),
+    "reset_csr_shard": (I32, [P, P, I32, I64, I32, I32, P, P, P, P]),
+    "reset_tc_count_shard": (I32, [P, P, P, I64, P, P, I64, P, P]),
+    "reset_sss_decide": (I32, [P, I32, P, P, I64, P, I32, I32, P, P, P]),
     "reset_gen_rmat": (I32, [I32, I32, C.c_uint64, C.c_double, C.c_double,
                              C.c_double, I32, C.POINTER(P), C.POINTER(P),
                              C.POINTER(I64), P]),

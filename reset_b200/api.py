@@ -252,11 +252,15 @@ def get_tuning() -> dict:
     t = Tuning()
     check(_lib().reset_get_tuning(C.byref(t)))
     return {"probe_rounds": t.probe_rounds, "warp_pair_min": t.warp_pair_min,
-            "probe_variant": t.probe_variant}
+            "probe_variant": t.probe_variant, "pair_method": t.pair_method}
+
+
+# reset_tuning.pair_method values
+PAIR_DEFAULT, PAIR_FLAT, PAIR_OWNER = 0, 1, 2
 
 
 def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] = None,
-               probe_variant: Optional[int] = None):
+               probe_variant: Optional[int] = None, pair_method: Optional[int] = None):
     t = Tuning()
     check(_lib().reset_get_tuning(C.byref(t)))
     if probe_rounds is not None:
@@ -265,6 +269,8 @@ def set_tuning(probe_rounds: Optional[int] = None, warp_pair_min: Optional[int] 
         t.warp_pair_min = warp_pair_min
     if probe_variant is not None:
         t.probe_variant = probe_variant
+    if pair_method is not None:
+        t.pair_method = pair_method
     check(_lib().reset_set_tuning(C.byref(t)))
 
 

@@ -12,7 +12,7 @@ namespace rst {
 static thread_local char g_err[512] = "";
 static std::atomic<long long> g_launches{0};
 static std::mutex g_tune_mu;
-static reset_tuning g_tune = {8, 64, 1, {0, 0, 0, 0, 0}};
+static reset_tuning g_tune = {8, 64, 1, 0, {0, 0, 0, 0}};
 
 reset_tuning tuning() {
   std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -102,6 +102,8 @@ reset_status reset_set_tuning(const reset_tuning* in) {
     return rst::arg_fail("warp_pair_min must be in 1..2^20");
   if (in->probe_variant != 0 && in->probe_variant != 1)
     return rst::arg_fail("probe_variant must be 0 or 1");
+  if (in->pair_method < 0 || in->pair_method > 2)
+    return rst::arg_fail("pair_method must be 0, 1 or 2");
   std::lock_guard<std::mutex> lock(rst::g_tune_mu);
   rst::g_tune = *in;
   return RESET_OK;

@@ -141,12 +141,38 @@ cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t st);
 reset_status tc_staged(const reset_table* t, const int4* desc,
                        const int32_t* d_cols, int64_t m,
                        unsigned long long* count, cudaStream_t st);
-// Owner-grouped triangle counting (tc_owner.cu): tables staged in shared
-// memory, probers' rows streamed with 16-byte loads (d_cols 16-byte
-// aligned); *count must be zeroed.
-reset_status tc_owner(const reset_table* t, const int4* desc, const int32_t* d_off,
-                      const int32_t* d_cols, const int32_t* chunk_rows, int64_t m,
+// Owner-grouped triangle counting (tc_owner.cu): sum over the edges (u, v)
+// of the edge CSR of |K(u) ∩ K(v)|, K = the key CSR t was built on (the
+// graph itself for plain TC); tables staged in shared memory, keys streamed
+// with 16-byte loads (kcols 16-byte aligned); *count must be zeroed.
+reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* koff,
+                      const int32_t* kcols, int64_t mk, const int32_t* eoff,
+                      const int32_t* ecols, const int32_t* echunk_rows, int64_t me,
                       unsigned long long* count, cudaStream_t st);
+// Owner-grouped pair decisions (sss_owner.cu).  Scratch for n sets and up to
+// `cap` pairs comes from one stream-ordered allocation.
+struct PairOwnerScratch {
+  int32_t *cnt = nullptr, *goff = nullptr, *pidx = nullptr, *wlist = nullptr,
+          *dlist = nullptr, *ctr = nullptr;
+  int2 *ent = nullptr, *units = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  void* base = nullptr;
+};
+reset_status pair_owner_alloc(int32_t n, int64_t cap, PairOwnerScratch* s, cudaStream_t st);
+void pair_owner_free(PairOwnerScratch* s, cudaStream_t st);
+// Decisions for the pairs p < cap (or p < *np_dev); elems 16-byte aligned,
+// cap <= INT32_MAX.  No allocation, no host synchronisation.
+reset_status pair_owner_launch(const reset_table* t, const int4* desc, const int32_t* elems,
+                               int64_t m, const int32_t* pa, const int32_t* pb, int64_t cap,
+                               const int64_t* np_dev, bool float_rule, int32_t num, int32_t den,
+                               float thr, uint8_t* flags, int32_t* inter,
+                               const PairOwnerScratch& s, cudaStream_t st);
+// pair_owner_alloc + launch + stream-ordered free.
+reset_status sss_owner(const reset_table* t, const int4* desc, const int32_t* elems, int64_t m,
+                       const int32_t* pa, const int32_t* pb, int64_t np, bool float_rule,
+                       int32_t num, int32_t den, float thr, uint8_t* flags, int32_t* inter,
+                       cudaStream_t st);
 // Counts launches of libreset's own kernels (reset_kernel_launches()).
 void note_launch(int k = 1);
 }  // namespace rst

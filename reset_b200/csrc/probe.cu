@@ -575,7 +575,7 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
     rows = owned_rows;
   }
   if (method == 3) {
-    reset_status s = tc_owner(t, ds.desc, d_off, d_cols, rows, m, cnt, st);
+    reset_status s = tc_owner(t, ds.desc, d_off, d_cols, m, d_off, d_cols, rows, m, cnt, st);
     if (owned_rows) cudaFreeAsync(owned_rows, st);
     return s;
   }
@@ -642,6 +642,12 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   DescScope ds;
   RST_CHECK(resolve_desc(t, d_off, st, &ds));
   const reset_tuning tun = tuning();
+  const bool el16 = (reinterpret_cast<uintptr_t>(d_elems) & 15) == 0;
+  if (tun.pair_method == 2 && !el16)
+    return arg_fail("pair_method 2 needs a 16-byte aligned element array");
+  if (tun.pair_method != 1 && el16 && np <= INT32_MAX)
+    return sss_owner(t, ds.desc, d_elems, t->m, d_pa, d_pb, np, float_rule, num, den, thr,
+                     d_flags, d_inter, st);
 #define SSS_LAUNCH(H, F, R, LN, ...)                                         \
   do {                                                                       \
     const int64_t g = clamp_grid(((np + 31) / 32 + kWarps - 1) / kWarps,     \

@@ -1,0 +1,255 @@
+// Device helpers of the owner-grouped probe kernels (tc_owner.cu,
+// sss_owner.cu): 1-D bulk copies of a set's table into shared memory
+// (cp.async.bulk completing on an mbarrier, with bounded waits), the
+// reference probe rule walked in the staged copy, and the flattened 16-byte
+// key streaming of up to 32 probing rows against one staged table.
+#pragma once
+
+#include "common.cuh"
+#include "probe_common.cuh"
+
+namespace rst {
+
+constexpr int kWaitLimit = 1 << 22;  // polls of a bulk-copy barrier before giving up
+
+// Launch shape and bins of the owner-grouped kernels.
+constexpr int kOT = 256;                 // threads per CTA
+constexpr int kOW = kOT / 32;            // warps per CTA
+constexpr int kCtaTab = 24576;           // ints of shared memory per CTA (96 KB)
+constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (3072 ints)
+constexpr int kCtaSeg = 512;             // probers per CTA work unit
+constexpr int kBigGroup = 256;           // groups above this are CTA work
+constexpr int kCtaWork = 32768;          // probes that make a smaller group CTA work
+
+// Bin of every owner w with a non-empty group ent[goff[w] .. goff[w+1])
+// ({row start, row length} of each prober): 0 = CTA work (units (w, seg)
+// of kCtaSeg probers), 1 = warp work, 2 = direct probes into the HBM table
+// (staging does not pay, or the table does not fit shared memory).
+// ctr[0..2] count the three lists.  Grid-stride over owners, block-uniform
+// loop (warp collectives inside).
+__device__ __forceinline__ void classify_owners(const int4* __restrict__ desc,
+                                                const int32_t* __restrict__ goff,
+                                                const int2* __restrict__ ent, int32_t n, int b,
+                                                int2* __restrict__ units,
+                                                int32_t* __restrict__ wlist,
+                                                int32_t* __restrict__ dlist,
+                                                int32_t* __restrict__ ctr) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+    const int64_t w = base + threadIdx.x;
+    int bin = -1, nunits = 0;
+    if (w < n) {
+      const int g0 = __ldg(goff + w), P = __ldg(goff + w + 1) - g0;
+      if (P > 0) {
+        const int64_t T = (int64_t)b << desc_lg(__ldg(desc + w));  // table ints
+        bool big = P > kBigGroup;
+        int64_t work = 0;
+        if (!big) {
+          for (int i = 0; i < P; ++i) work += __ldg(&ent[g0 + i].y);
+          big = work >= kCtaWork;
+        }
+        // staging pays when the table has at most ~4 ints per probe
+        const bool stage = T <= kCtaTab && (P > kBigGroup || T <= 4 * work);
+        if (!stage) {
+          bin = 2;
+        } else if (big || T > kWarpTab) {
+          bin = 0;
+          nunits = (P + kCtaSeg - 1) / kCtaSeg;
+        } else {
+          bin = 1;
+        }
+      }
+    }
+    // warp-aggregated appends
+    {
+      int tot;
+      const int pre = warp_excl_scan(bin == 0 ? nunits : 0, &tot);
+      int b0 = 0;
+      if (lane == 0 && tot) b0 = atomicAdd(ctr + 0, tot);
+      b0 = __shfl_sync(kFull, b0, 0);
+      for (int s = 0; s < nunits; ++s) units[b0 + pre + s] = make_int2((int)w, s);
+    }
+#pragma unroll
+    for (int which = 1; which <= 2; ++which) {
+      const unsigned bm = __ballot_sync(kFull, bin == which);
+      int b0 = 0;
+      if (lane == 0 && bm) b0 = atomicAdd(ctr + which, __popc(bm));
+      b0 = __shfl_sync(kFull, b0, 0);
+      if (bin == which) (which == 1 ? wlist : dlist)[b0 + __popc(bm & lanemask_lt())] = (int)w;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before
+// later bulk copies into it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity`; false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Issues the bulk copies of one set's table (b planes of 1 << lg ints, plane
+// k at table + toff + k*bn in HBM) into S, plane k at S + k * (1 << lg).
+__device__ __forceinline__ void stage_table(int* S, const int32_t* __restrict__ table,
+                                            int64_t toff, int lg, int64_t bn, int b,
+                                            uint64_t* bar) {
+  const int L = 1 << lg;
+  const uint32_t plane = (uint32_t)L * 4u;
+  fence_proxy_async_smem();
+  mbar_expect_tx(bar, plane * (uint32_t)b);
+  for (int k = 0; k < b; ++k) bulk_g2s(S + (int64_t)k * L, table + toff + k * bn, plane, bar);
+}
+
+// Continues search_in_hashtable (TC.cu:11-31) in a staged table (plane k at
+// S + k*L) after slot 0 of bucket h held another key.  Same bound as
+// probe_key (the whole table).
+__device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h, int b,
+                                              int32_t* status) {
+  int k = 1;
+  const int cap = L * b;
+  for (int t = 1; t < cap; ++t) {
+    if (k == b) {
+      k = 0;
+      h = (h + 1) & (L - 1);
+    }
+    const int s = S[k * L + h];
+    if (s == x) return 1;
+    if (s == -1) return 0;
+    ++k;
+  }
+  atomicOr(status, kErrProbeLimit);
+  return 0;
+}
+
+// The keys of up to 32 probing rows (lane i: ent[i] = {row start, row
+// length} in cols) looked up in one staged table.  The rows' 16-byte chunks
+// are flattened across the lanes (round r: lane i loads chunk 32r+i of the
+// concatenation, its row found by a shuffle binary search) and R rounds are
+// in flight at once.  Returns this lane's hits; with PAIRS, the hits of row
+// i are also added to s_cnt[i] (32 shared-memory counters of this warp,
+// zeroed by the caller), reduced over the lanes of each row first.
+template <bool HIER, int R, bool PAIRS = false>
+__device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
+                                                const int32_t* __restrict__ cols, int64_t m,
+                                                const int* S, int lg, int lg_max, int b,
+                                                int32_t* status, int* s_cnt = nullptr) {
+  const int lane = threadIdx.x & 31;
+  const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
+  const int64_t end = (int64_t)e.x + e.y;
+  const int nc = e.y > 0 ? (int)(((end + 3) >> 2) - (e.x >> 2)) : 0;
+  int total;
+  const int P = warp_excl_scan(nc, &total);
+  const int L = 1 << lg;
+  const unsigned hmask = HIER ? ((1u << lg_max) - 1u) : (unsigned)(L - 1);
+  const int hsh = HIER ? (lg_max - lg) : 0;
+  const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
+  const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
+  unsigned hits = 0;
+  for (int base = 0; base < total; base += 32 * R) {
+    int x[R][4];
+    unsigned vm[R];  // bit j: element j of this lane's chunk belongs to the row
+    int kk[R];       // the row (lane index) of this lane's chunk, -1 if none
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      vm[r] = 0;
+      kk[r] = -1;
+      x[r][0] = x[r][1] = x[r][2] = x[r][3] = 0;
+      if (base + r * 32 < total) {  // warp-uniform
+        const int f = base + r * 32 + lane;
+        const int k = owner_lane(P, f);
+        const int kp = __shfl_sync(kFull, P, k);
+        const int kb = __shfl_sync(kFull, e.x, k);
+        const int kd = __shfl_sync(kFull, e.y, k);
+        if (f < total) {
+          kk[r] = k;
+          const int64_t c = (int64_t)(kb >> 2) + (f - kp);
+          const int64_t i0 = c * 4;
+          const int lo = (int)max((int64_t)kb - i0, (int64_t)0);
+          const int hi = (int)min((int64_t)kb + kd - i0, (int64_t)4);
+          vm[r] = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+          if (c < full4) {
+            const int4 q = __ldg(cols4 + c);
+            x[r][0] = q.x;
+            x[r][1] = q.y;
+            x[r][2] = q.z;
+            x[r][3] = q.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if ((vm[r] >> j) & 1u) x[r][j] = __ldg(cols + i0 + j);
+          }
+        }
+      }
+    }
+    int h[R][4], s0[R][4];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        h[r][j] = (int)(((unsigned)x[r][j] & hmask) >> hsh);
+        s0[r][j] = ((vm[r] >> j) & 1u) ? S[h[r][j]] : -1;
+      }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      unsigned hr = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!((vm[r] >> j) & 1u)) continue;
+        if (s0[r][j] == x[r][j]) {
+          ++hr;
+        } else if (s0[r][j] != -1) {
+          hr += smem_walk(x[r][j], S, L, h[r][j], b, status);
+        }
+      }
+      hits += hr;
+      if (PAIRS && base + r * 32 < total) {  // warp-uniform
+        const unsigned grp = __match_any_sync(kFull, kk[r]);
+        const unsigned sum = __reduce_add_sync(grp, hr);
+        if (kk[r] >= 0 && lane == __ffs(grp) - 1 && sum) atomicAdd(s_cnt + kk[r], (int)sum);
+      }
+    }
+  }
+  return hits;
+}
+
+}  // namespace rst

@@ -414,16 +414,16 @@ extern "C" reset_status reset_tc_count_noalloc(const reset_table* t,
   if (m > 0 && !d_cols) return arg_fail("NULL cols");
   if (d_off && d_off != t->build_off)
     return arg_fail("reset_tc_count_noalloc needs the offsets the table was built from");
-  // the kernel walks rows through the table's build-time descriptors, so the
-  // column array must be the one of the build CSR (same length)
-  if (m != t->m)
-    return arg_fail("reset_tc_count_noalloc needs m equal to the table's edge count");
   if (m > kNoAllocMaxEdges || t->m > kNoAllocMaxEdges) {
     set_error("invalid argument: reset_tc_count_noalloc takes at most %lld edges "
               "(its fixed scratch holds %d work units)",
               (long long)kNoAllocMaxEdges, kNoAllocUnits);
     return RESET_ERR_ARG;
   }
+  // the kernel walks rows through the table's build-time descriptors, so the
+  // column array must be the one of the build CSR (same length)
+  if (m != t->m)
+    return arg_fail("reset_tc_count_noalloc needs m equal to the table's edge count");
   cudaStream_t st = as_stream(stream);
   int2* scratch = nullptr;
   RST_CHECK(noalloc_scratch(&scratch));

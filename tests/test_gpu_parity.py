@@ -194,6 +194,48 @@ def test_sss_random_pairs_and_empty_sets(R, cuda, oracle_mod):
         assert np.array_equal(host(f), of)
 
 
+@pytest.mark.parametrize("hier", [True, False])
+def test_sss_pair_methods_agree(R, cuda, oracle_mod, hier):
+    """The owner-grouped pair path (tables staged in shared memory, every bin:
+    CTA units with more than 512 probers, warp owners, direct owners with
+    tables too large to stage) and the pair-flattened path give the oracle's
+    sizes and decisions, integer and float rule, with and without sizes, on
+    sets with repeated entries (the probe direction matters there)."""
+    rng = np.random.default_rng(11)
+    sizes = rng.integers(0, 120, size=3000)
+    sizes[::23] = 0
+    sizes[:4] = [9000, 3000, 700, 2048]          # 9000 keys: table too large to stage
+    off, elems = _synthetic_csr(rng, sizes, 20000)
+    # repeated entries in every 5th set
+    rows = [elems[off[u]:off[u + 1]] for u in range(sizes.size)]
+    rows = [np.concatenate([r, r[: r.size // 4]]) if u % 5 == 0 else r for u, r in enumerate(rows)]
+    off = np.concatenate([[0], np.cumsum([r.size for r in rows])]).astype(np.int32)
+    elems = np.concatenate(rows).astype(np.int32)
+    P = 60000
+    pa = rng.integers(0, sizes.size, size=P).astype(np.int32)
+    pb = rng.integers(0, sizes.size, size=P).astype(np.int32)
+    pa[:4000] = rng.integers(0, 4, size=4000)     # ~1000 probers for each big set
+    pb[4000:4100] = pa[4000:4100]
+    doff, de, dpa, dpb = (dev(x, cuda) for x in (off, elems, pa, pb))
+    t = R.Table(doff, de, hierarchical=hier)
+    ot = oracle_mod.Table(off, elems, hier=hier)
+    of, oi = oracle_mod.sss(ot, pa, pb, mode=1, num=3, den=10)
+    off_f, _ = oracle_mod.sss(ot, pa, pb, mode=0, thr=0.3)
+    before = R.get_tuning()
+    try:
+        for method in (R.PAIR_OWNER, R.PAIR_FLAT, R.PAIR_DEFAULT):
+            R.set_tuning(pair_method=method)
+            f, i = R.sss(t, doff, de, dpa, dpb, 3, 10)
+            assert np.array_equal(host(i), oi) and np.array_equal(host(f), of), method
+            f, _ = R.sss(t, doff, de, dpa, dpb, 3, 10, with_inter=False)
+            assert np.array_equal(host(f), of), method
+            f, _ = R.sss_float(t, doff, de, dpa, dpb, 0.3)
+            assert np.array_equal(host(f), off_f), method
+        t.check()
+    finally:
+        R.set_tuning(**before)
+
+
 # -------------------------------------------------------------------- IR --
 
 def _ir_index(rng, nterms, ndocs, npost, nq, empty_every=0):
