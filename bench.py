@@ -107,6 +107,8 @@ def parse():
                     help="length of each Poisson arrival phase")
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--max-batch", type=int, default=1024)
+    ap.add_argument("--max-batch-cost", type=int, default=1 << 22,
+                    help="served forms: estimated probes per batch at most (0 = no limit)")
     return ap.parse_args()
 
 

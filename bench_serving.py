@@ -387,7 +387,7 @@ def ir_serve_ours(a, rank, world, local):
     ix_holder = {}
 
     def factory(streams, mb):
-        srv = Server(streams=streams, max_batch_requests=mb)
+        srv = Server(streams=streams, max_batch_requests=mb, max_batch_cost=a.max_batch_cost)
         ix_holder["ix"] = srv.add_index(t)
         return srv
 
@@ -425,6 +425,7 @@ def ir_serve_ours(a, rank, world, local):
                    "df_law": f"Zipf(1.1), df(1) = {a.df_max}", "query_terms": "2-6, by df",
                    "mean_terms": qterms, "burst_requests": a.requests,
                    "streams": a.streams, "max_batch": a.max_batch,
+                   "max_batch_cost": a.max_batch_cost,
                    "mean_batch_in_burst": st["mean_batch"],
                    "capacity_client": "closed loop, 4096 requests outstanding",
                    "server_counters_after_burst": st,
@@ -584,7 +585,7 @@ def mixed_serve_ours(a, rank, world, local):
     ixs = {}
 
     def factory(streams, mb):
-        srv = Server(streams=streams, max_batch_requests=mb)
+        srv = Server(streams=streams, max_batch_requests=mb, max_batch_cost=a.max_batch_cost)
         ixs["o"] = srv.add_index(to)
         ixs["s"] = srv.add_index(ts)
         return srv
@@ -640,6 +641,7 @@ def mixed_serve_ours(a, rank, world, local):
                    "triples": "1-16 triangles (u,v,w) per job -> |N(u)∩N(v)∩N(w)|",
                    "raw": "|A|,|B| log-uniform over 2^4..2^20, ids in [0, 2^22)",
                    "streams": a.streams, "max_batch": a.max_batch,
+                   "max_batch_cost": a.max_batch_cost,
                    "mean_batch_in_burst": st["mean_batch"], "checked_exactly": checked,
                    "server_counters_after_burst": st,
                    "parallelism": f"replicas x{world}"},

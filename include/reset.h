@@ -380,7 +380,12 @@ typedef struct {
   int32_t max_batch_requests; /* requests per batch at most (default 1024)    */
   int64_t mem_budget_bytes;   /* device bytes for batches; 0 = half the free
                                  device memory when the server starts        */
-  int32_t reserved[8];
+  int64_t max_batch_cost;     /* estimated probes per batch at most (default
+                                 2^22; 0 = no limit).  A request above it runs
+                                 in a batch of its own, and such batches hold
+                                 at most streams - 1 slots, so lighter requests
+                                 never wait behind one (they may pass it)   */
+  int32_t reserved[6];
 } reset_server_config;
 
 enum {
@@ -468,11 +473,10 @@ typedef struct reset_tuning {
   int32_t warp_pair_min; /* pairs with >= this many keys get a whole warp   */
   int32_t probe_variant; /* whole-warp pair loop: 0 = software-pipelined,
                             1 = lean (branch-free resolve, no prefetch)     */
-  int32_t pair_method;   /* reset_sss / reset_sss_float: 0 = default
-                            (owner-grouped when the elements are 16-byte
-                            aligned), 1 = pair-flattened (with early exit
-                            when deciding only), 2 = owner-grouped (tables
-                            staged in shared memory)                         */
+  int32_t pair_method;   /* reset_sss / reset_sss_float: 0 = default (1),
+                            1 = pair-flattened (with early exit when
+                            deciding only), 2 = owner-grouped (tables staged
+                            in shared memory; 16-byte aligned elements)      */
   int32_t reserved[4];
 } reset_tuning;
 

@@ -154,7 +154,7 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
 struct PairOwnerScratch {
   int32_t *cnt = nullptr, *goff = nullptr, *pidx = nullptr, *wlist = nullptr,
           *dlist = nullptr, *ctr = nullptr;
-  int2 *ent = nullptr, *units = nullptr;
+  int2 *ent = nullptr, *units = nullptr, *dunits = nullptr;
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
   void* base = nullptr;

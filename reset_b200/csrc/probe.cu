@@ -560,7 +560,7 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   const bool cols16 = (reinterpret_cast<uintptr_t>(d_cols) & 15) == 0;
   if (method == 3 && !cols16)
     return arg_fail("method 3 needs a 16-byte aligned column array");
-  if (method == 0) method = cols16 ? 3 : 1;
+  if (method == 0) method = cols16 && m <= INT32_MAX - 4 ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
@@ -645,7 +645,9 @@ static reset_status sss_common(const reset_table* t, const int32_t* d_off,
   const bool el16 = (reinterpret_cast<uintptr_t>(d_elems) & 15) == 0;
   if (tun.pair_method == 2 && !el16)
     return arg_fail("pair_method 2 needs a 16-byte aligned element array");
-  if (tun.pair_method != 1 && el16 && np <= INT32_MAX)
+  // default: the pair-flattened kernel (measured faster or equal on B200 for
+  // graph pairs and self-join candidates, and it stops deciding pairs early)
+  if (tun.pair_method == 2 && el16 && np <= INT32_MAX && t->m <= INT32_MAX - 4)
     return sss_owner(t, ds.desc, d_elems, t->m, d_pa, d_pb, np, float_rule, num, den, thr,
                      d_flags, d_inter, st);
 #define SSS_LAUNCH(H, F, R, LN, ...)                                         \

@@ -196,6 +196,7 @@ struct Req {
   std::vector<int32_t> a, b;
   int64_t t_arr = 0, t_start = 0, t_done = 0;
   int64_t dev_bytes = 0;
+  int64_t cost = 0;  // estimated probes (batch formation)
   int64_t aux = 0;  // IR: df(first term); TC: number of (v, w) pairs; RAW: len
   reset_status status = RESET_OK;
   BlockP docs_block;               // IR: survivors live in this pinned block, or
@@ -258,6 +259,7 @@ struct Batch {
   int64_t reserved = 0;
   int64_t t_launch = 0;
   int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
+  bool heavy = false;  // one request above the cost cap
   BlockP res;     // pinned block receiving the IR survivors (phase 1), or
   const int32_t* res_ptr = nullptr;  // the slot's own buffer (then copied out)
   reset_status status = RESET_OK;
@@ -290,7 +292,7 @@ struct reset_server {
   bool stop = false;
   std::thread worker;
   int64_t n_done = 0, n_batches = 0, sum_batch = 0, max_batch = 0;
-  int64_t max_in_use = 0, max_inflight = 0, inflight = 0;
+  int64_t max_in_use = 0, max_inflight = 0, inflight = 0, heavy_inflight = 0;
   int64_t launch_ns = 0, batch_ns = 0;
   std::vector<BlockP> blocks;  // pinned result blocks (free when only the pool holds one)
 };
@@ -314,6 +316,8 @@ reset_status plan_request(const reset_server* s, Req* r) {
       r->aux = df;
       const int64_t ns = (df + slice - 1) / slice;
       r->dev_bytes = 4 * (int64_t)r->a.size() + 32 + 4 * df + (4 * slice + 12) * ns;
+      // the first list is read and probed against each further term
+      r->cost = df * std::max<int64_t>(1, (int64_t)r->a.size() - 1);
       break;
     }
     case RESET_REQ_PAIRS: {
@@ -323,6 +327,9 @@ reset_status plan_request(const reset_server* s, Req* r) {
       for (int32_t v : r->a)
         if (v < 0 || v >= ix.n()) return arg_fail("set id out of range");
       r->dev_bytes = 13 * (int64_t)(r->a.size() / 2);
+      for (size_t i = 0; i + 1 < r->a.size(); i += 2)
+        r->cost += 1 + std::min(ix.h_off[r->a[i] + 1] - ix.h_off[r->a[i]],
+                                ix.h_off[r->a[i + 1] + 1] - ix.h_off[r->a[i + 1]]);
       break;
     }
     case RESET_REQ_TRIPLES: {
@@ -331,6 +338,12 @@ reset_status plan_request(const reset_server* s, Req* r) {
       for (int32_t v : r->a)
         if (v < 0 || v >= ix.n()) return arg_fail("set id out of range");
       r->dev_bytes = 16 * (int64_t)(r->a.size() / 3);
+      for (size_t i = 0; i + 2 < r->a.size(); i += 3) {
+        int64_t lo = INT64_MAX;
+        for (int j = 0; j < 3; ++j)
+          lo = std::min(lo, (int64_t)(ix.h_off[r->a[i + j] + 1] - ix.h_off[r->a[i + j]]));
+        r->cost += 1 + 2 * lo;
+      }
       break;
     }
     case RESET_REQ_TC_VERTEX: {
@@ -338,7 +351,9 @@ reset_status plan_request(const reset_server* s, Req* r) {
       int64_t P = 0;
       for (int32_t v : r->a) {
         if (v < 0 || v >= ix.n()) return arg_fail("vertex out of range");
-        P += ix.h_off[v + 1] - ix.h_off[v];
+        const int64_t d = ix.h_off[v + 1] - ix.h_off[v];
+        P += d;
+        r->cost += 1 + d * std::min<int64_t>(d, 256);  // each (v, w) probes <= d keys
       }
       r->aux = P;
       r->dev_bytes = 12 * (int64_t)r->a.size() + 13 * P;
@@ -353,6 +368,7 @@ reset_status plan_request(const reset_server* s, Req* r) {
         if (x < 0) return arg_fail("raw keys must be >= 0");
       r->aux = calc_len((int)nb, 0.2f, 5);
       r->dev_bytes = 4 * (int64_t)(r->a.size() + nb) + 20 * r->aux + 16;
+      r->cost = (int64_t)r->a.size() + nb;
       break;
     }
     default:
@@ -835,6 +851,7 @@ void worker_main(reset_server* s) {
       }
       s->in_use -= bt->reserved;
       --s->inflight;
+      if (bt->heavy) --s->heavy_inflight;
       progressed = true;
       s->cv_done.notify_all();
     }
@@ -842,26 +859,51 @@ void worker_main(reset_server* s) {
     for (auto& sl : s->slots) {
       if (sl.batch || s->pending.empty()) continue;
       auto bt = std::make_unique<Batch>();
-      int64_t bytes = 0;
-      while (!s->pending.empty() &&
-             (int64_t)bt->reqs.size() < s->cfg.max_batch_requests) {
-        ReqP& r = s->pending.front();
+      int64_t bytes = 0, cost = 0;
+      // Requests are taken in arrival order while the batch's estimated
+      // probes stay under the cap.  A request above the cap is "heavy": it
+      // runs alone, and only while another slot stays open for the rest;
+      // when it cannot start, lighter requests behind it (within a window)
+      // may pass it.
+      const int64_t cap = s->cfg.max_batch_cost > 0 ? s->cfg.max_batch_cost : INT64_MAX;
+      const bool heavy_room = s->slots.size() == 1 ||
+                              s->heavy_inflight + 1 < (int64_t)s->slots.size();
+      int passed = 0;
+      for (auto it = s->pending.begin();
+           it != s->pending.end() && (int64_t)bt->reqs.size() < s->cfg.max_batch_requests;) {
+        ReqP r = *it;
         if (r->dev_bytes > s->budget) {  // can never fit: fail it
           r->status = RESET_ERR_OOM;
           r->t_done = now_ns();
           r->done = true;
           ++s->n_done;
-          s->pending.pop_front();
+          it = s->pending.erase(it);
           progressed = true;
           s->cv_done.notify_all();
           continue;
         }
+        if (r->cost > cap) {
+          if (bt->reqs.empty() && heavy_room) {
+            if (s->in_use + r->dev_bytes > s->budget) break;  // wait for memory
+            bytes = r->dev_bytes;
+            bt->reqs.push_back(r);
+            bt->heavy = true;
+            it = s->pending.erase(it);
+            break;
+          }
+          if (!bt->reqs.empty() || ++passed > 64) break;  // a light batch ends here
+          ++it;  // pass the heavy request it cannot start now
+          continue;
+        }
+        if (!bt->reqs.empty() && cost + r->cost > cap) break;
         if (s->in_use + bytes + r->dev_bytes > s->budget) break;  // wait for memory
         bytes += r->dev_bytes;
+        cost += r->cost;
         bt->reqs.push_back(r);
-        s->pending.pop_front();
+        it = s->pending.erase(it);
       }
-      if (bt->reqs.empty()) break;
+      if (bt->reqs.empty()) continue;
+      if (bt->heavy) ++s->heavy_inflight;
       bt->id = s->next_batch++;
       bt->reserved = bytes;
       s->in_use += bytes;
@@ -909,6 +951,7 @@ void reset_server_config_default(reset_server_config* c) {
   std::memset(c, 0, sizeof(*c));
   c->streams = 4;
   c->max_batch_requests = 1024;
+  c->max_batch_cost = int64_t(1) << 22;
   c->mem_budget_bytes = 0;
 }
 
@@ -923,6 +966,7 @@ reset_status reset_server_create(const reset_server_config* cfg, reset_server** 
   if (c.streams < 1 || c.streams > 64) return arg_fail("streams must be in 1..64");
   if (c.max_batch_requests < 1) return arg_fail("max_batch_requests must be >= 1");
   if (c.mem_budget_bytes < 0) return arg_fail("negative memory budget");
+  if (c.max_batch_cost < 0) return arg_fail("negative max_batch_cost");
   std::unique_ptr<reset_server> s;
   try {
     s.reset(new reset_server());

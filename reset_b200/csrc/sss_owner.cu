@@ -110,8 +110,9 @@ __global__ void __launch_bounds__(kOT)
     pair_classify_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
                          const int2* __restrict__ ent, int32_t n, int b,
                          int2* __restrict__ units, int32_t* __restrict__ wlist,
-                         int32_t* __restrict__ dlist, int32_t* __restrict__ ctr) {
-  classify_owners(desc, goff, ent, n, b, units, wlist, dlist, ctr);
+                         int32_t* __restrict__ dlist, int2* __restrict__ dunits,
+                         int32_t* __restrict__ ctr) {
+  classify_owners(desc, goff, ent, n, b, units, wlist, dlist, dunits, ctr);
 }
 
 template <bool FLOAT_RULE>
@@ -135,27 +136,30 @@ __global__ void __launch_bounds__(kOT, 2)
                      const int2* __restrict__ ent, const int32_t* __restrict__ pidx,
                      const int32_t* __restrict__ elems, int64_t m,
                      const int2* __restrict__ units, const int32_t* __restrict__ wlist,
-                     const int32_t* __restrict__ dlist, int32_t* __restrict__ ctr,
+                     const int32_t* __restrict__ dlist, const int2* __restrict__ dunits,
+                     int32_t* __restrict__ ctr,
                      const int32_t* __restrict__ table, int64_t bn, int b, int lg_max,
                      int num, int den, float thr, uint8_t* __restrict__ flags,
                      int32_t* __restrict__ inter, int32_t* __restrict__ status) {
   extern __shared__ __align__(128) int sm[];
   __shared__ __align__(8) uint64_t s_bar[kOW + 1];
   __shared__ int s_item, s_next;
+  __shared__ int s_qx[kOW][kQueue], s_qh[kOW][kQueue];
   __shared__ int s_cnt[kOW][32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= kOW) mbar_init(&s_bar[tid]);
   fence_mbar_init();
   __syncthreads();
   uint32_t par_cta = 0, par_warp = 0;
-  const int n_units = ctr[0], n_warp = ctr[1], n_direct = ctr[2];
+  const int n_units = ctr[0], n_warp = ctr[1], n_direct = ctr[2], n_dunits = ctr[6];
   int* C = s_cnt[warp];
 
   // one batch of up to 32 probers of owner w (length dw), table staged at S
   auto batch = [&](int g, int c, const int* S, int lg, int dw) {
     C[lane] = 0;
     __syncwarp();
-    staged_keys<HIER, R, true>(ent + g, c, elems, m, S, lg, lg_max, b, status, C);
+    staged_keys<HIER, R, true>(ent + g, c, elems, m, S, lg, lg_max, b, status, s_qx[warp],
+                               s_qh[warp], C);
     __syncwarp();
     if (lane < c)
       decide<FLOAT_RULE>(__ldg(pidx + g + lane), C[lane], __ldg(&ent[g + lane].y), dw, num,
@@ -193,6 +197,31 @@ __global__ void __launch_bounds__(kOT, 2)
       batch(g, min(32, g1 - g), sm, lg, dw.y);
     }
     __syncthreads();
+  }
+
+  // ---- direct units: up to kDirSeg pairs of one owner whose table stays in
+  // HBM, 32 pairs at a time, their probes flattened across the lanes
+  for (;;) {
+    int ui = 0;
+    if (lane == 0) ui = atomicAdd(ctr + 7, 1);
+    ui = __shfl_sync(kFull, ui, 0);
+    if (ui >= n_dunits) break;
+    const int2 unit = __ldg(dunits + ui);
+    const int4 dw = __ldg(desc + unit.x);
+    const int g0 = __ldg(goff + unit.x) + unit.y * kDirSeg;
+    const int g1 = min(__ldg(goff + unit.x + 1), g0 + kDirSeg);
+    for (int g = g0; g < g1; g += 32) {
+      const int gi = g + lane;
+      const int2 e = gi < g1 ? __ldg(ent + gi) : make_int2(0, 0);
+      C[lane] = 0;
+      __syncwarp();
+      flat_probe<HIER>(elems, m, table, e.y, e.x, desc_toff(dw), desc_lg(dw), lg_max, bn, b,
+                       status, [&](int kk) { atomicAdd(C + kk, 1); });
+      __syncwarp();
+      if (gi < g1)
+        decide<FLOAT_RULE>(__ldg(pidx + gi), C[lane], e.y, dw.y, num, den, thr, flags, inter);
+      __syncwarp();
+    }
   }
 
   // ---- warp owners
@@ -277,9 +306,10 @@ reset_status pair_owner_alloc(int32_t n, int64_t cap, PairOwnerScratch* s, cudaS
   const size_t sz_n1 = al(sizeof(int32_t) * ((size_t)n + 1));
   const size_t sz_ent = al(sizeof(int2) * c), sz_pidx = al(sizeof(int32_t) * c);
   const size_t sz_units = al(sizeof(int2) * ((size_t)n + c / kCtaSeg + 1));
+  const size_t sz_dunits = al(sizeof(int2) * ((size_t)n + c / kDirSeg + 1));
   const size_t sz_list = al(sizeof(int32_t) * ((size_t)n + 1)), sz_ctr = al(sizeof(int32_t) * 8);
-  const size_t total = 2 * sz_n1 + sz_ent + sz_pidx + sz_units + 2 * sz_list + sz_ctr +
-                       al(s->cub_bytes);
+  const size_t total = 2 * sz_n1 + sz_ent + sz_pidx + sz_units + sz_dunits + 2 * sz_list +
+                       sz_ctr + al(s->cub_bytes);
   char* p = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&p), total, st));
   s->base = p;
@@ -290,6 +320,7 @@ reset_status pair_owner_alloc(int32_t n, int64_t cap, PairOwnerScratch* s, cudaS
   s->units = reinterpret_cast<int2*>(p); p += sz_units;
   s->wlist = reinterpret_cast<int32_t*>(p); p += sz_list;
   s->dlist = reinterpret_cast<int32_t*>(p); p += sz_list;
+  s->dunits = reinterpret_cast<int2*>(p); p += sz_dunits;
   s->ctr = reinterpret_cast<int32_t*>(p); p += sz_ctr;
   s->cub_tmp = p;
   return RESET_OK;
@@ -310,6 +341,7 @@ reset_status pair_owner_launch(const reset_table* t, const int4* desc, const int
                                float thr, uint8_t* flags, int32_t* inter,
                                const PairOwnerScratch& s, cudaStream_t st) {
   const int32_t n = t->n;
+  if (m > INT32_MAX - 4) return arg_fail("owner-grouped pairs take at most 2^31 - 5 elements");
   const int sms = sm_count();
   RST_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int32_t) * ((size_t)n + 1), st));
   RST_CUDA(cudaMemsetAsync(s.ctr, 0, sizeof(int32_t) * 8, st));
@@ -326,7 +358,8 @@ reset_status pair_owner_launch(const reset_table* t, const int4* desc, const int
   RST_CUDA(cudaGetLastError());
   note_launch();
   pair_classify_kernel<<<blocks(n, sms * 8), kOT, 0, st>>>(desc, s.goff, s.ent, n, t->bucket,
-                                                           s.units, s.wlist, s.dlist, s.ctr);
+                                                           s.units, s.wlist, s.dlist, s.dunits,
+                                                           s.ctr);
   RST_CUDA(cudaGetLastError());
   const size_t smem = sizeof(int) * kCtaTab;
 #define SO_KERNEL(H, F) sss_owner_kernel<H, F, 4>
@@ -341,7 +374,7 @@ reset_status pair_owner_launch(const reset_table* t, const int4* desc, const int
   note_launch();
 #define SO_LAUNCH(H, F)                                                                   \
   SO_KERNEL(H, F)<<<grid, kOT, smem, st>>>(desc, s.goff, s.ent, s.pidx, elems, m, s.units, \
-                                           s.wlist, s.dlist, s.ctr, t->d_table,          \
+                                           s.wlist, s.dlist, s.dunits, s.ctr, t->d_table, \
                                            t->bucket_num, t->bucket, t->lg_max, num, den,  \
                                            thr, flags, inter, t->d_status)
   if (t->hier) {

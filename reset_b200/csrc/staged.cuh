@@ -13,26 +13,30 @@ namespace rst {
 constexpr int kWaitLimit = 1 << 22;  // polls of a bulk-copy barrier before giving up
 
 // Launch shape and bins of the owner-grouped kernels.
-constexpr int kOT = 256;                 // threads per CTA
+constexpr int kOT = 512;                 // threads per CTA (2 CTAs, 32 warps per SM)
 constexpr int kOW = kOT / 32;            // warps per CTA
 constexpr int kCtaTab = 24576;           // ints of shared memory per CTA (96 KB)
 constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (3072 ints)
 constexpr int kCtaSeg = 512;             // probers per CTA work unit
 constexpr int kBigGroup = 256;           // groups above this are CTA work
 constexpr int kCtaWork = 32768;          // probes that make a smaller group CTA work
+constexpr int kDirSeg = 256;             // probers per direct work unit
 
 // Bin of every owner w with a non-empty group ent[goff[w] .. goff[w+1])
 // ({row start, row length} of each prober): 0 = CTA work (units (w, seg)
 // of kCtaSeg probers), 1 = warp work, 2 = direct probes into the HBM table
-// (staging does not pay, or the table does not fit shared memory).
-// ctr[0..2] count the three lists.  Grid-stride over owners, block-uniform
-// loop (warp collectives inside).
+// (staging does not pay, or the table does not fit shared memory) for
+// groups of at most 32 probers, 3 = the same for larger groups, cut into
+// units (w, seg) of kDirSeg probers so that no warp serialises a hub's
+// whole group.  ctr[0..2] and ctr[6] count the four lists.  Grid-stride
+// over owners, block-uniform loop (warp collectives inside).
 __device__ __forceinline__ void classify_owners(const int4* __restrict__ desc,
                                                 const int32_t* __restrict__ goff,
                                                 const int2* __restrict__ ent, int32_t n, int b,
                                                 int2* __restrict__ units,
                                                 int32_t* __restrict__ wlist,
                                                 int32_t* __restrict__ dlist,
+                                                int2* __restrict__ dunits,
                                                 int32_t* __restrict__ ctr) {
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -52,7 +56,8 @@ __device__ __forceinline__ void classify_owners(const int4* __restrict__ desc,
         // staging pays when the table has at most ~4 ints per probe
         const bool stage = T <= kCtaTab && (P > kBigGroup || T <= 4 * work);
         if (!stage) {
-          bin = 2;
+          bin = P > 32 ? 3 : 2;
+          if (bin == 3) nunits = (P + kDirSeg - 1) / kDirSeg;
         } else if (big || T > kWarpTab) {
           bin = 0;
           nunits = (P + kCtaSeg - 1) / kCtaSeg;
@@ -62,13 +67,17 @@ __device__ __forceinline__ void classify_owners(const int4* __restrict__ desc,
       }
     }
     // warp-aggregated appends
-    {
+#pragma unroll
+    for (int which = 0; which <= 3; which += 3) {
       int tot;
-      const int pre = warp_excl_scan(bin == 0 ? nunits : 0, &tot);
+      const int pre = warp_excl_scan(bin == which ? nunits : 0, &tot);
+      int* c = ctr + (which == 0 ? 0 : 6);
       int b0 = 0;
-      if (lane == 0 && tot) b0 = atomicAdd(ctr + 0, tot);
+      if (lane == 0 && tot) b0 = atomicAdd(c, tot);
       b0 = __shfl_sync(kFull, b0, 0);
-      for (int s = 0; s < nunits; ++s) units[b0 + pre + s] = make_int2((int)w, s);
+      int2* u = which == 0 ? units : dunits;
+      if (bin == which)
+        for (int s = 0; s < nunits; ++s) u[b0 + pre + s] = make_int2((int)w, s);
     }
 #pragma unroll
     for (int which = 1; which <= 2; ++which) {
@@ -141,13 +150,12 @@ __device__ __forceinline__ void stage_table(int* S, const int32_t* __restrict__ 
 }
 
 // Continues search_in_hashtable (TC.cu:11-31) in a staged table (plane k at
-// S + k*L) after slot 0 of bucket h held another key.  Same bound as
-// probe_key (the whole table).
-__device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h, int b,
+// S + k*L) from slot k of bucket h (k == b: the next bucket's slot 0); the
+// slots before it held other keys.  Same bound as probe_key (the table).
+__device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h, int k, int b,
                                               int32_t* status) {
-  int k = 1;
   const int cap = L * b;
-  for (int t = 1; t < cap; ++t) {
+  for (int t = 0; t < cap; ++t) {
     if (k == b) {
       k = 0;
       h = (h + 1) & (L - 1);
@@ -161,19 +169,28 @@ __device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h,
   return 0;
 }
 
+constexpr int kQueue = 128;  // pending probes a warp queues per round (32 lanes x 4 keys)
+
 // The keys of up to 32 probing rows (lane i: ent[i] = {row start, row
 // length} in cols) looked up in one staged table.  The rows' 16-byte chunks
 // are flattened across the lanes (round r: lane i loads chunk 32r+i of the
 // concatenation, its row found by a shuffle binary search) and R rounds are
-// in flight at once.  Returns this lane's hits; with PAIRS, the hits of row
-// i are also added to s_cnt[i] (32 shared-memory counters of this warp,
-// zeroed by the caller), reduced over the lanes of each row first.
+// in flight at once.  Every key's first two probe slots (slots 0 and 1 of
+// its home bucket; with one slot per bucket, the home and next bucket) are
+// read and resolved without branching; probes that both slots leave open are
+// queued in this warp's shared-memory queue (qx, qh: kQueue entries each)
+// and walked by all lanes together, so the rare long walks do not idle the
+// warp.  Returns this lane's hits; with PAIRS, the hits of row i are also
+// added to s_cnt[i] (32 shared-memory counters of this warp, zeroed by the
+// caller).
 template <bool HIER, int R, bool PAIRS = false>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
-                                                int32_t* status, int* s_cnt = nullptr) {
+                                                int32_t* status, int* qx, int* qh,
+                                                int* s_cnt = nullptr) {
   const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
   const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
   const int64_t end = (int64_t)e.x + e.y;
   const int nc = e.y > 0 ? (int)(((end + 3) >> 2) - (e.x >> 2)) : 0;
@@ -182,6 +199,10 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   const int L = 1 << lg;
   const unsigned hmask = HIER ? ((1u << lg_max) - 1u) : (unsigned)(L - 1);
   const int hsh = HIER ? (lg_max - lg) : 0;
+  // the second probe slot and where a queued walk continues
+  const int off1 = b > 1 ? L : 0;   // slot 1 of the home bucket, or ...
+  const int inc1 = b > 1 ? 0 : 1;   // ... slot 0 of the next bucket
+  const int kcont = b > 1 ? 2 : 1;  // the slot of bucket h1 a queued walk continues at
   const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
   const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
   unsigned hits = 0;
@@ -202,10 +223,11 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         const int kd = __shfl_sync(kFull, e.y, k);
         if (f < total) {
           kk[r] = k;
-          const int64_t c = (int64_t)(kb >> 2) + (f - kp);
-          const int64_t i0 = c * 4;
-          const int lo = (int)max((int64_t)kb - i0, (int64_t)0);
-          const int hi = (int)min((int64_t)kb + kd - i0, (int64_t)4);
+          // m <= 2^31 - 5 (checked on the host): 4c + 3 fits an int
+          const int c = (kb >> 2) + (f - kp);
+          const int i0 = c * 4;
+          const int lo = max(kb - i0, 0);
+          const int hi = min(kb + kd - i0, 4);
           vm[r] = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
           if (c < full4) {
             const int4 q = __ldg(cols4 + c);
@@ -221,28 +243,46 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         }
       }
     }
-    int h[R][4], s0[R][4];
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        h[r][j] = (int)(((unsigned)x[r][j] & hmask) >> hsh);
-        s0[r][j] = ((vm[r] >> j) & 1u) ? S[h[r][j]] : -1;
-      }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
+      if (base + r * 32 >= total) break;  // warp-uniform
       unsigned hr = 0;
+      int nq = 0;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        if (!((vm[r] >> j) & 1u)) continue;
-        if (s0[r][j] == x[r][j]) {
-          ++hr;
-        } else if (s0[r][j] != -1) {
-          hr += smem_walk(x[r][j], S, L, h[r][j], b, status);
+        const bool act = (vm[r] >> j) & 1u;
+        const int xx = x[r][j];
+        const int h = (int)(((unsigned)xx & hmask) >> hsh);
+        const int h1 = (h + inc1) & (L - 1);
+        const int s0 = act ? S[h] : -1;
+        const int s1 = act ? S[off1 + h1] : -1;
+        const bool m0 = s0 == xx, e0 = s0 == -1, m1 = s1 == xx, e1 = s1 == -1;
+        hr += (unsigned)(act & (m0 | (!e0 & m1)));
+        const bool pend = act & !m0 & !e0 & !m1 & !e1;
+        const unsigned pm = __ballot_sync(kFull, pend);
+        if (pend) {
+          // continue at slot 2 of the home bucket (or, one slot per bucket,
+          // at the bucket after h1); the row rides along for PAIRS
+          qx[nq + __popc(pm & lt)] = xx;
+          qh[nq + __popc(pm & lt)] = (h1 << 10) | (kcont << 5) | kk[r];
         }
+        nq += __popc(pm);
+      }
+      if (nq) {
+        __syncwarp();
+        for (int i = lane; i < nq; i += 32) {
+          const int v = qh[i];
+          const unsigned hit = smem_walk(qx[i], S, L, v >> 10, (v >> 5) & 31, b, status);
+          if (PAIRS) {
+            if (hit) atomicAdd(s_cnt + (v & 31), 1);
+          } else {
+            hits += hit;
+          }
+        }
+        __syncwarp();
       }
       hits += hr;
-      if (PAIRS && base + r * 32 < total) {  // warp-uniform
+      if (PAIRS) {
         const unsigned grp = __match_any_sync(kFull, kk[r]);
         const unsigned sum = __reduce_add_sync(grp, hr);
         if (kk[r] >= 0 && lane == __ffs(grp) - 1 && sum) atomicAdd(s_cnt + kk[r], (int)sum);

@@ -129,13 +129,15 @@ __global__ void __launch_bounds__(kOT)
 }
 
 // Bin of every owner with a non-empty group (see the file comment).
-// ctr[0] CTA units, ctr[1] warp owners, ctr[2] direct owners.
+// ctr[0] CTA units, ctr[1] warp owners, ctr[2] small direct owners,
+// ctr[6] direct units.
 __global__ void __launch_bounds__(kOT)
     own_classify_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
                         const int2* __restrict__ ent, int32_t n, int b,
                         int2* __restrict__ units, int32_t* __restrict__ wlist,
-                        int32_t* __restrict__ dlist, int32_t* __restrict__ ctr) {
-  classify_owners(desc, goff, ent, n, b, units, wlist, dlist, ctr);
+                        int32_t* __restrict__ dlist, int2* __restrict__ dunits,
+                        int32_t* __restrict__ ctr) {
+  classify_owners(desc, goff, ent, n, b, units, wlist, dlist, dunits, ctr);
 }
 
 template <bool HIER, int R>
@@ -143,19 +145,21 @@ __global__ void __launch_bounds__(kOT, 2)
     tc_owner_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
                     const int2* __restrict__ ent, const int32_t* __restrict__ cols, int64_t m,
                     const int2* __restrict__ units, const int32_t* __restrict__ wlist,
-                    const int32_t* __restrict__ dlist, int32_t* __restrict__ ctr,
+                    const int32_t* __restrict__ dlist, const int2* __restrict__ dunits,
+                    int32_t* __restrict__ ctr,
                     const int32_t* __restrict__ table, int64_t bn, int b, int lg_max,
                     unsigned long long* __restrict__ count, int32_t* __restrict__ status) {
   extern __shared__ __align__(128) int sm[];
   __shared__ __align__(8) uint64_t s_bar[kOW + 1];
   __shared__ int s_item, s_next;
+  __shared__ int s_qx[kOW][kQueue], s_qh[kOW][kQueue];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= kOW) mbar_init(&s_bar[tid]);
   fence_mbar_init();
   __syncthreads();
   unsigned long long hits = 0;
   uint32_t par_cta = 0, par_warp = 0;
-  const int n_units = ctr[0], n_warp = ctr[1], n_direct = ctr[2];
+  const int n_units = ctr[0], n_warp = ctr[1], n_direct = ctr[2], n_dunits = ctr[6];
 
   // ---- CTA units: the whole CTA stages one table, warps share its probers
   for (;;) {
@@ -184,9 +188,28 @@ __global__ void __launch_bounds__(kOT, 2)
       if (lane == 0) g = g0 + atomicAdd(&s_next, 32);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, sm, lg, lg_max, b, status);
+      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, sm, lg, lg_max, b, status,
+                                   s_qx[warp], s_qh[warp]);
     }
     __syncthreads();
+  }
+
+  // ---- direct units: up to kDirSeg probers of one owner whose table stays
+  // in HBM, 32 probers at a time, their probes flattened across the lanes
+  for (;;) {
+    int ui = 0;
+    if (lane == 0) ui = atomicAdd(ctr + 7, 1);
+    ui = __shfl_sync(kFull, ui, 0);
+    if (ui >= n_dunits) break;
+    const int2 unit = __ldg(dunits + ui);
+    const int4 dw = __ldg(desc + unit.x);
+    const int g0 = __ldg(goff + unit.x) + unit.y * kDirSeg;
+    const int g1 = min(__ldg(goff + unit.x + 1), g0 + kDirSeg);
+    for (int g = g0; g < g1; g += 32) {
+      const int2 e = g + lane < g1 ? __ldg(ent + g + lane) : make_int2(0, 0);
+      hits += flat_probe<HIER>(cols, m, table, e.y, e.x, desc_toff(dw), desc_lg(dw), lg_max,
+                               bn, b, status, [](int) {});
+    }
   }
 
   // ---- warp owners: each warp stages a table in its own region
@@ -210,7 +233,8 @@ __global__ void __launch_bounds__(kOT, 2)
     }
     const int g0 = __ldg(goff + w), g1 = __ldg(goff + w + 1);
     for (int g = g0; g < g1; g += 32)
-      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, W, lg, lg_max, b, status);
+      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, W, lg, lg_max, b, status,
+                                   s_qx[warp], s_qh[warp]);
   }
 
   // ---- direct owners: 32 owners per warp, their (owner, prober) pairs
@@ -267,17 +291,20 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   const int64_t n = t->n;
   const int64_t m = me;
   if (n == 0 || me == 0 || mk == 0) return RESET_OK;
-  // scratch, one allocation: cnt/left, goff, ent, units, wlist, dlist, ctr, CUB
+  if (mk > INT32_MAX - 4) return arg_fail("the owner-grouped count takes at most 2^31 - 5 keys");
+  // scratch, one allocation: cnt/left, goff, ent, units, wlist, dlist, dunits,
+  // ctr, CUB
   size_t cub_bytes = 0;
   RST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (int32_t*)nullptr,
                                          (int32_t*)nullptr, (int)(n + 1), st));
-  const int64_t max_units = n + m / kCtaSeg + 1;
+  const int64_t max_units = n + m / kCtaSeg + 1, max_dunits = n + m / kDirSeg + 1;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t sz_cnt = al(sizeof(int32_t) * (n + 1)), sz_goff = sz_cnt;
   const size_t sz_ent = al(sizeof(int2) * m), sz_units = al(sizeof(int2) * max_units);
   const size_t sz_list = al(sizeof(int32_t) * n), sz_ctr = al(sizeof(int32_t) * 8);
-  const size_t total = sz_cnt + sz_goff + sz_ent + sz_units + 2 * sz_list + sz_ctr +
-                       al(cub_bytes);
+  const size_t sz_dunits = al(sizeof(int2) * max_dunits);
+  const size_t total = sz_cnt + sz_goff + sz_ent + sz_units + 2 * sz_list + sz_dunits +
+                       sz_ctr + al(cub_bytes);
   char* base = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&base), total, st));
   char* p = base;
@@ -287,6 +314,7 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   int2* units = reinterpret_cast<int2*>(p); p += sz_units;
   int32_t* wlist = reinterpret_cast<int32_t*>(p); p += sz_list;
   int32_t* dlist = reinterpret_cast<int32_t*>(p); p += sz_list;
+  int2* dunits = reinterpret_cast<int2*>(p); p += sz_dunits;
   int32_t* ctr = reinterpret_cast<int32_t*>(p); p += sz_ctr;
   void* cub_tmp = p;
 
@@ -312,7 +340,7 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   if (e == cudaSuccess) {
     note_launch();
     own_classify_kernel<<<grid_stride_blocks((n + kOT - 1) / kOT, sms * 8), kOT, 0, st>>>(
-        kdesc, goff, ent, t->n, t->bucket, units, wlist, dlist, ctr);
+        kdesc, goff, ent, t->n, t->bucket, units, wlist, dlist, dunits, ctr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
@@ -327,11 +355,13 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
       note_launch();
       if (t->hier)
         tc_owner_kernel<true, 4><<<grid, kOT, smem, st>>>(
-            kdesc, goff, ent, kcols, mk, units, wlist, dlist, ctr, t->d_table, t->bucket_num,
+            kdesc, goff, ent, kcols, mk, units, wlist, dlist, dunits, ctr, t->d_table,
+            t->bucket_num,
             t->bucket, t->lg_max, count, t->d_status);
       else
         tc_owner_kernel<false, 4><<<grid, kOT, smem, st>>>(
-            kdesc, goff, ent, kcols, mk, units, wlist, dlist, ctr, t->d_table, t->bucket_num,
+            kdesc, goff, ent, kcols, mk, units, wlist, dlist, dunits, ctr, t->d_table,
+            t->bucket_num,
             t->bucket, t->lg_max, count, t->d_status);
       e = cudaGetLastError();
     }

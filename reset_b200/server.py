@@ -46,13 +46,15 @@ def _i32(a) -> np.ndarray:
 
 class Server:
     def __init__(self, streams: int = 4, max_batch_requests: int = 1024,
-                 mem_budget_bytes: int = 0):
+                 mem_budget_bytes: int = 0, max_batch_cost: Optional[int] = None):
         L = load()
         cfg = ServerConfig()
         L.reset_server_config_default(C.byref(cfg))
         cfg.streams = streams
         cfg.max_batch_requests = max_batch_requests
         cfg.mem_budget_bytes = mem_budget_bytes
+        if max_batch_cost is not None:   # estimated probes per batch; 0 = no limit
+            cfg.max_batch_cost = max_batch_cost
         h = C.c_void_p()
         check(L.reset_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
