@@ -662,9 +662,92 @@ def mixed_serve_ours(a, rank, world, local):
 
 # ============================================================== dispatch ==
 
+# =============================================================== tc-batch ==
+
+SEED_TCB = 0x5EED0BA0
+
+
+def tc_batch_ours(a, rank, world, local):
+    """Batched TC: `graphs` disjoint seeded R-MAT graphs (scales cycling
+    over 8..12), counted (1) by the plain per-call form -- per graph one
+    table build and one reset_tc_count, each waited for -- and (2) batched:
+    one block-diagonal CSR, one table build and one reset_tc_count_batch.
+    Per-graph counts must be equal; both timed with CUDA events."""
+    torch = _setup(local, world)
+    from reset_b200 import api, _lib
+    L = _lib.load()
+    scales = [8 + (i % 5) for i in range(a.graphs)]
+    gs = [api.gen_rmat(s, 16, SEED_TCB + i, oriented=True) for i, s in enumerate(scales)]
+    nv = [int(o.numel() - 1) for o, _ in gs]
+    ne = [int(c.numel()) for _, c in gs]
+    vb = np.concatenate([[0], np.cumsum(nv)]).astype(np.int64)
+    eb = np.concatenate([[0], np.cumsum(ne)]).astype(np.int64)
+    off = torch.cat([torch.zeros(1, dtype=torch.int64, device="cuda")] +
+                    [o[1:].long() + int(eb[i]) for i, (o, _) in enumerate(gs)]).int()
+    cols = torch.cat([c.long() + int(vb[i]) for i, (_, c) in enumerate(gs)]).int()
+    gro = torch.tensor(vb, dtype=torch.int32, device="cuda")
+    m = int(cols.numel())
+    alpha, bucket = 0.2, 5
+
+    def plain():
+        out = []
+        for o, c in gs:
+            t = api.Table(o, c, alpha=alpha, bucket=bucket, hierarchical=True, hash_order=True)
+            out.append(api.tc_count(t, o, t.hash_order))
+            t.free()
+        return out
+
+    def batched():
+        t = api.Table(off, cols, alpha=alpha, bucket=bucket, hierarchical=True, hash_order=True)
+        r = api.tc_count_batch(t, off, t.hash_order, gro)
+        t.free_async()
+        return r
+
+    def timed(fn, reps):
+        ms, res = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms), res
+
+    for _ in range(a.warmup):
+        want = plain()
+        batched()
+    l0 = L.reset_kernel_launches()
+    with B.Clocks(local) as clk:
+        ms_b, got = timed(batched, a.steps)
+    launches = L.reset_kernel_launches() - l0
+    ms_p, want = timed(plain, max(1, min(a.steps, 3)))
+    assert got.cpu().tolist() == want, "batched per-graph counts differ from per-call counts"
+    ms_b, ms_p = _maxr([ms_b, ms_p], world)
+    line = {
+        "metric": "TC edges/sec, batched (many graphs per launch) vs plain per-call",
+        "value": world * m / (ms_b / 1e3), "unit": "edges/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT graphs generated on device)",
+        "config": {"workload": f"tc_batch_{a.graphs}_rmat_s8_12", "graphs": a.graphs,
+                   "vertices": int(vb[-1]), "oriented_edges": m,
+                   "triangles": int(sum(want)), "alpha": alpha, "bucket": bucket,
+                   "parity": "per-graph counts of the batched call equal the per-call counts",
+                   "parallelism": f"replicas x{world}"},
+        "plain_per_call": {"value": world * m / (ms_p / 1e3), "unit": "edges/s",
+                           "ms_per_pass": ms_p,
+                           "note": "per graph: table build + reset_tc_count, each waited for"},
+        "speedup_vs_plain": ms_p / ms_b,
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    _finish(line, rank, world)
+
+
 def run_ours(a, rank, world, local):
     {"sss-join": sss_join_ours, "ir-serve": ir_serve_ours,
-     "mixed-serve": mixed_serve_ours}[a.workload](a, rank, world, local)
+     "mixed-serve": mixed_serve_ours, "tc-batch": tc_batch_ours}[a.workload](a, rank, world, local)
 
 
 def run_reference(a, rank, world):
@@ -703,6 +786,18 @@ def run_reference(a, rank, world):
         reqs = _ir_queries(np.diff(toff).astype(np.int64), 5000, rng)
         cb = _ir_cpu(toff, docs, reqs, a.cpu_seconds)
         unit, metric = "queries/s", "IR queries/sec"
+    elif a.workload == "tc-batch":
+        t0 = time.perf_counter()
+        edges, gi = 0, 0
+        while time.perf_counter() - t0 < a.cpu_seconds and gi < a.graphs:
+            o, c = oracle.rmat_graph(8 + (gi % 5), 16, SEED_TCB + gi, oriented=True)
+            oracle.tc_merge(o, c, nthreads=1)
+            edges += int(c.size)
+            gi += 1
+        el = time.perf_counter() - t0
+        cb = {"value": edges / el, "unit": "edges/s", "cores": 1, "kind": "port",
+              "sample": f"{gi} of the {a.graphs} graphs, oracle merge TC one by one, {el:.1f} s"}
+        unit, metric = "edges/s", "TC edges/sec, batched (many graphs per launch) vs plain per-call"
     else:
         off, cols = oracle.rmat_graph(18, 16, SEED_MIX, oriented=False)
         rng = np.random.default_rng(SEED_MIX)

@@ -171,6 +171,21 @@ reset_status reset_tc_count_ex(const reset_table *t, const int32_t *d_off,
  * keeps the last call's contents (the counters are cleared at every call):
  * calls that overlap on the GPU -- on different streams, or from different
  * threads -- race on it and must be serialised by the caller. */
+/* Batched triangle counting: n_graphs disjoint oriented graphs stored as
+ * one block-diagonal CSR (graph g owns the vertices
+ * d_graph_off[g] .. d_graph_off[g+1] - 1; d_graph_off[0] = 0, nondecreasing,
+ * d_graph_off[n_graphs] = n; edges stay inside their graph) with one table.
+ * d_counts[g] (device u64) receives graph g's triangle count -- the
+ * reference's dynamic_triangle_count (triangle-count/TC.cu:128-190) run once
+ * per graph -- from a single owner-grouped count over the whole batch (each
+ * triangle is credited to the graph of the vertex whose table it is found
+ * in).  d_off/m must be the CSR the table was built on and d_cols 16-byte
+ * aligned.  No host synchronisation. */
+reset_status reset_tc_count_batch(const reset_table *t, const int32_t *d_off,
+                                  const int32_t *d_cols, int64_t m,
+                                  const int32_t *d_graph_off, int32_t n_graphs,
+                                  uint64_t *d_counts, reset_stream_t stream);
+
 reset_status reset_tc_count_noalloc(const reset_table *t, const int32_t *d_off,
                                     const int32_t *d_cols, int64_t m,
                                     uint64_t *d_count, reset_stream_t stream);
@@ -270,6 +285,18 @@ reset_status reset_ir(const reset_table *t, const int32_t *d_toff,
 reset_status reset_clique4_count(const reset_table *t, const int32_t *d_off,
                                  const int32_t *d_cols, int64_t m,
                                  uint64_t *d_count, reset_stream_t stream);
+
+/* k-cliques, 3 <= k <= 16, of an oriented graph whose table is `t` (built
+ * on d_off/d_cols): SMOG's clique DFS (DFSKernelForClique,
+ * SMOG/SMOG_hie/subgraph_match_hie.cu:58-247) with every candidate set
+ * C_{j+1} = C_j ∩ N+(w) found by hash probes, starting from
+ * C_0 = N+(u) ∩ N+(v) for every edge (u, v); each clique is counted once.
+ * k = 3 gives the triangle count, k = 4 the 4-clique count.  *d_count
+ * (device u64) is overwritten.  Synchronises `stream` once (scratch
+ * sizing: k - 3 rows of the largest out-degree per warp). */
+reset_status reset_clique_count(const reset_table *t, const int32_t *d_off,
+                                const int32_t *d_cols, int64_t m, int32_t k,
+                                uint64_t *d_count, reset_stream_t stream);
 
 /* |A ∩ B| counted with A's multiplicity for one pair of device arrays
  * (keys >= 0).  Builds B's table with `params` and probes A.  *d_count

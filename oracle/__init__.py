@@ -86,6 +86,8 @@ def lib():
         L.ro_jaccard_join.restype = C.c_int64
         L.ro_clique4.argtypes = [C.c_int32, _i32p, _i32p]
         L.ro_clique4.restype = C.c_uint64
+        L.ro_clique_k.argtypes = [C.c_int32, _i32p, _i32p, C.c_int32]
+        L.ro_clique_k.restype = C.c_uint64
         L.ro_relabel.argtypes = [C.c_uint64, C.c_int32, C.c_uint32]
         L.ro_relabel.restype = C.c_uint32
         L.ro_mix64.argtypes = [C.c_uint64]
@@ -219,6 +221,14 @@ def clique4(off, cols) -> int:
     off = _c(off, np.int32)
     cols = _c(cols, np.int32)
     return int(lib().ro_clique4(off.size - 1, off, cols if cols.size else np.zeros(1, np.int32)))
+
+
+def clique_k(off, cols, k: int) -> int:
+    """k-cliques (k >= 3) of an oriented graph with sorted rows (ro_clique_k)."""
+    off = _c(off, np.int32)
+    cols = _c(cols, np.int32)
+    return int(lib().ro_clique_k(off.size - 1, off, cols if cols.size else np.zeros(1, np.int32),
+                                 k))
 
 
 def jaccard_join(off, tok, num=7, den=10):

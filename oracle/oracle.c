@@ -449,6 +449,54 @@ uint64_t ro_clique4(int32_t n, const int32_t *off, const int32_t *cols) {
   return total;
 }
 
+/* k-cliques of an oriented graph with sorted rows: the clique search of
+ * SMOG's DFSKernelForClique (SMOG/SMOG_hie/subgraph_match_hie.cu:58-247),
+ * where the candidates of level l+1 are those of level l intersected with
+ * the out-row of the vertex picked at level l (orientation breaks the
+ * symmetry, so every clique is counted once).  Depth-first, candidate sets
+ * by sorted merge; level 2 starts from every edge (u, v). */
+static uint64_t ro_clique_level(const int32_t *off, const int32_t *cols, int32_t *buf,
+                                int32_t maxd, const int32_t *C, int32_t nc, int32_t left) {
+  /* left: vertices still to pick from C */
+  if (left == 1) return (uint64_t)nc;
+  uint64_t total = 0;
+  int32_t *D = buf;
+  for (int32_t t = 0; t < nc; t++) {
+    const int32_t w = C[t];
+    int32_t a = 0, b = off[w], nd = 0;
+    while (a < nc && b < off[w + 1]) {
+      if (C[a] < cols[b]) a++;
+      else if (C[a] > cols[b]) b++;
+      else { D[nd++] = C[a]; a++; b++; }
+    }
+    total += ro_clique_level(off, cols, buf + maxd, maxd, D, nd, left - 1);
+  }
+  return total;
+}
+
+uint64_t ro_clique_k(int32_t n, const int32_t *off, const int32_t *cols, int32_t k) {
+  if (k < 3) return 0;
+  int32_t maxd = 1;
+  for (int32_t u = 0; u < n; u++)
+    if (off[u + 1] - off[u] > maxd) maxd = off[u + 1] - off[u];
+  int32_t *buf = (int32_t *)malloc(sizeof(int32_t) * (size_t)maxd * (size_t)(k - 1));
+  uint64_t total = 0;
+  for (int32_t u = 0; u < n; u++) {
+    for (int32_t e = off[u]; e < off[u + 1]; e++) {
+      const int32_t v = cols[e];
+      int32_t i = off[u], j = off[v], nw = 0;
+      while (i < off[u + 1] && j < off[v + 1]) {
+        if (cols[i] < cols[j]) i++;
+        else if (cols[i] > cols[j]) j++;
+        else { buf[nw++] = cols[i]; i++; j++; }
+      }
+      total += ro_clique_level(off, cols, buf + maxd, maxd, buf, nw, k - 2);
+    }
+  }
+  free(buf);
+  return total;
+}
+
 /* ------------------------------------------------------------------------ */
 /* synthetic inputs                                                          */
 /* ------------------------------------------------------------------------ */

@@ -114,6 +114,9 @@ int64_t ro_jaccard_join(int32_t n, const int32_t *off, const int32_t *tok,
 
 /* 4-cliques of an oriented graph with sorted rows (merge intersections). */
 uint64_t ro_clique4(int32_t n, const int32_t *off, const int32_t *cols);
+/* k-cliques (k >= 3) of an oriented graph with sorted rows, each counted
+ * once (SMOG/SMOG_hie/subgraph_match_hie.cu:58-247). */
+uint64_t ro_clique_k(int32_t n, const int32_t *off, const int32_t *cols, int32_t k);
 
 /* ---- synthetic inputs --------------------------------------------------- */
 

@@ -96,7 +96,9 @@ SIGNATURES = {
     "reset_tc_count": (I32, [P, P, P, I64, P, P]),
     "reset_tc_count_ex": (I32, [P, P, P, I64, I32, P, P]),
     "reset_tc_count_noalloc": (I32, [P, P, P, I64, P, P]),
+    "reset_tc_count_batch": (I32, [P, P, P, I64, P, I32, P, P]),
     "reset_clique4_count": (I32, [P, P, P, I64, P, P]),
+    "reset_clique_count": (I32, [P, P, P, I64, I32, P, P]),
     "reset_sss": (I32, [P, P, P, P, P, I64, I32, I32, P, P, P]),
     "reset_sss_float": (I32, [P, P, P, P, P, I64, C.c_float, P, P, P]),
     "reset_ir": (I32, [P, P, P, P, P, I32, P, P, P, P]),

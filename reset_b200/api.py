@@ -169,6 +169,28 @@ def clique4_count(t: Table, off: torch.Tensor, cols: torch.Tensor, stream=None) 
     return int(out.item()) & ((1 << 64) - 1)
 
 
+def tc_count_batch(t: Table, off: torch.Tensor, cols: torch.Tensor, graph_off: torch.Tensor,
+                   out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+    """Per-graph triangle counts of disjoint graphs in one block-diagonal
+    CSR (graph g owns vertices graph_off[g] .. graph_off[g+1]-1) -> int64
+    tensor of len(graph_off) - 1 counts, asynchronously."""
+    g = graph_off.numel() - 1
+    _need(graph_off, torch.int32, "graph_off")
+    if out is None:
+        out = torch.empty(g, dtype=torch.int64, device=cols.device)
+    check(_lib().reset_tc_count_batch(t.handle, _ptr(off), _ptr(cols), cols.numel(),
+                                      _ptr(graph_off), g, _ptr(out), _stream(stream)))
+    return out
+
+
+def clique_count(t: Table, off: torch.Tensor, cols: torch.Tensor, k: int, stream=None) -> int:
+    """k-cliques (3 <= k <= 16) of the oriented graph the table was built on."""
+    out = torch.zeros(1, dtype=torch.int64, device=cols.device)
+    check(_lib().reset_clique_count(t.handle, _ptr(off), _ptr(cols), cols.numel(), k,
+                                    _ptr(out), _stream(stream)))
+    return int(out.item()) & ((1 << 64) - 1)
+
+
 def sss(t: Table, off, elems, pa, pb, num: int = 7, den: int = 10,
         with_inter: bool = True, stream=None):
     """Integer-rule set-similarity decisions -> (flags uint8, inter int32)."""

@@ -144,11 +144,13 @@ reset_status tc_staged(const reset_table* t, const int4* desc,
 // Owner-grouped triangle counting (tc_owner.cu): sum over the edges (u, v)
 // of the edge CSR of |K(u) ∩ K(v)|, K = the key CSR t was built on (the
 // graph itself for plain TC); tables staged in shared memory, keys streamed
-// with 16-byte loads (kcols 16-byte aligned); *count must be zeroed.
+// with 16-byte loads (kcols 16-byte aligned); *count must be zeroed.  With
+// owner_hits (n zeroed u64), every owner's hits are also added there.
 reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* koff,
                       const int32_t* kcols, int64_t mk, const int32_t* eoff,
                       const int32_t* ecols, const int32_t* echunk_rows, int64_t me,
-                      unsigned long long* count, cudaStream_t st);
+                      unsigned long long* count, cudaStream_t st,
+                      unsigned long long* owner_hits = nullptr);
 // Owner-grouped pair decisions (sss_owner.cu).  Scratch for n sets and up to
 // `cap` pairs comes from one stream-ordered allocation.
 struct PairOwnerScratch {

@@ -413,7 +413,7 @@ reset_status ir_run(const reset_table* t, const int4* desc, const int32_t* docs,
                     const int64_t* sl_off, int64_t total_slices,
                     const int64_t* res_off, int32_t* res, int32_t* stage,
                     int32_t* sl_cnt, int64_t* pos, int32_t* cnt,
-                    int64_t* packed_off, cudaStream_t st);
+                    int64_t* packed_off, cudaStream_t st, bool yield);
 
 int persistent_grid(const void* kernel) {
   int per_sm = 0;
@@ -433,10 +433,15 @@ reset_status ir_run(const reset_table* t, const int4* desc, const int32_t* docs,
                     const int64_t* sl_off, int64_t total_slices,
                     const int64_t* res_off, int32_t* res, int32_t* stage,
                     int32_t* sl_cnt, int64_t* pos, int32_t* cnt,
-                    int64_t* packed_off, cudaStream_t st) {
+                    int64_t* packed_off, cudaStream_t st, bool yield) {
+  // yield: one warp per slice and no persistent grid, so the blocks retire
+  // as they finish and the block scheduler can interleave other streams'
+  // (higher-priority) work; otherwise a persistent grid walks the slices
+  const int64_t per_slice = std::min<int64_t>((total_slices + kWarps - 1) / kWarps, INT32_MAX);
   if (total_slices > 0) {
-    const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,
-                                 persistent_grid((const void*)ir_slice_kernel<HIER>));
+    const int64_t g = yield ? per_slice
+                            : clamp_grid(per_slice,
+                                         persistent_grid((const void*)ir_slice_kernel<HIER>));
     note_launch();
     ir_slice_kernel<HIER><<<(int)g, kThreads, 0, st>>>(
         desc, t->n, docs, query, qoff, nq, sl_off, stage, sl_cnt, t->d_table,
@@ -447,8 +452,8 @@ reset_status ir_run(const reset_table* t, const int4* desc, const int32_t* docs,
   slice_scan_kernel<<<1, 1024, 0, st>>>(sl_cnt, total_slices, pos);
   RST_CUDA(cudaGetLastError());
   if (total_slices > 0) {
-    const int64_t g = clamp_grid((total_slices + kWarps - 1) / kWarps,
-                                 persistent_grid((const void*)ir_gather_kernel));
+    const int64_t g = yield ? per_slice
+                            : clamp_grid(per_slice, persistent_grid((const void*)ir_gather_kernel));
     note_launch();
     ir_gather_kernel<<<(int)g, kThreads, 0, st>>>(sl_off, nq, sl_cnt, pos, stage, res_off,
                                                    res);
@@ -535,13 +540,13 @@ reset_status ir_launch_planned(const reset_table* t, const int32_t* docs,
                                int64_t total_slices, const int64_t* res_off,
                                int32_t* res, int32_t* stage, int32_t* sl_cnt,
                                int64_t* pos, int32_t* cnt, int64_t* packed_off,
-                               cudaStream_t st) {
+                               cudaStream_t st, bool yield) {
   if (nq <= 0) return RESET_OK;
   if (t->hier)
     return ir_run<true>(t, t->d_desc, docs, query, qoff, nq, sl_off, total_slices, res_off,
-                        res, stage, sl_cnt, pos, cnt, packed_off, st);
+                        res, stage, sl_cnt, pos, cnt, packed_off, st, yield);
   return ir_run<false>(t, t->d_desc, docs, query, qoff, nq, sl_off, total_slices, res_off,
-                       res, stage, sl_cnt, pos, cnt, packed_off, st);
+                       res, stage, sl_cnt, pos, cnt, packed_off, st, yield);
 }
 
 }  // namespace rst
@@ -789,9 +794,9 @@ reset_status reset_ir(const reset_table* t, const int32_t* d_toff,
   IR_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_stage),
                           sizeof(int32_t) * (size_t)(total > 0 ? total : 1) * kIrSlice, st));
   rs = t->hier ? ir_run<true>(t, ds.desc, d_docs, d_query, d_qoff, nq, d_sl, total, d_res_off,
-                              d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st)
+                              d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st, false)
                : ir_run<false>(t, ds.desc, d_docs, d_query, d_qoff, nq, d_sl, total, d_res_off,
-                               d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st);
+                               d_res, d_stage, d_slc, d_pos, d_cnt, nullptr, st, false);
   if (rs != RESET_OK) {
     cleanup();
     return rs;

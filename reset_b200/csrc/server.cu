@@ -40,7 +40,7 @@ reset_status ir_launch_planned(const reset_table* t, const int32_t* docs,
                                int64_t total_slices, const int64_t* res_off,
                                int32_t* res, int32_t* stage, int32_t* sl_cnt,
                                int64_t* pos, int32_t* cnt, int64_t* packed_off,
-                               cudaStream_t st);
+                               cudaStream_t st, bool yield = false);
 int ir_slice_size();
 }  // namespace rst
 
@@ -260,13 +260,15 @@ struct Batch {
   int64_t t_launch = 0;
   int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
   bool heavy = false;  // one request above the cost cap
+  cudaStream_t st = nullptr;  // the slot stream the batch runs on
   BlockP res;     // pinned block receiving the IR survivors (phase 1), or
   const int32_t* res_ptr = nullptr;  // the slot's own buffer (then copied out)
   reset_status status = RESET_OK;
 };
 
 struct Slot {
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;     // light batches (highest priority)
+  cudaStream_t st_lo = nullptr;  // heavy batches (lowest priority)
   cudaEvent_t ev = nullptr;
   Pinned in, out, res;
   void* arena = nullptr;  // device buffer reused by this slot's batches
@@ -592,7 +594,8 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   }
 
   // ---- device work
-  cudaStream_t st = sl.st;
+  bt.st = bt.heavy ? sl.st_lo : sl.st;
+  cudaStream_t st = bt.st;
   if (bt.d_bytes > sl.arena_cap) {  // grow (stream-ordered; the slot is idle)
     if (sl.arena) RST_CUDA(cudaFreeAsync(sl.arena, st));
     sl.arena = nullptr;
@@ -617,7 +620,7 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
             reinterpret_cast<int32_t*>(dp + g.sc[0]),
             reinterpret_cast<int64_t*>(dp + g.sc3),
             reinterpret_cast<int32_t*>(dp + g.out[0]),
-            reinterpret_cast<int64_t*>(dp + g.out[1]), st));
+            reinterpret_cast<int64_t*>(dp + g.out[1]), st, /*yield=*/bt.heavy));
         break;
       }
       case RESET_REQ_PAIRS: {
@@ -805,13 +808,13 @@ bool enqueue_results(reset_server* s, Slot& sl, Batch& bt) {
     if (g.kind != RESET_REQ_IR || g.dense_n == 0) continue;
     cudaError_t e = cudaMemcpyAsync(const_cast<int32_t*>(bt.res_ptr) + g.dense_host,
                                     dp + g.sc[2], 4 * (size_t)g.dense_n,
-                                    cudaMemcpyDeviceToHost, sl.st);
+                                    cudaMemcpyDeviceToHost, bt.st);
     if (e != cudaSuccess) {
       bt.status = cuda_fail(e, "result copy", __FILE__, __LINE__);
       return false;
     }
   }
-  cudaError_t e = cudaEventRecord(sl.ev, sl.st);
+  cudaError_t e = cudaEventRecord(sl.ev, bt.st);
   if (e != cudaSuccess) {
     bt.status = cuda_fail(e, "cudaEventRecord", __FILE__, __LINE__);
     return false;
@@ -925,7 +928,7 @@ void worker_main(reset_server* s) {
       const int64_t t_launched = now_ns();
       if (rs != RESET_OK) {
         bt->status = rs;
-        cudaEventRecord(sl.ev, sl.st);  // completes once the slot drains
+        cudaEventRecord(sl.ev, bt->st ? bt->st : sl.st);  // completes once the slot drains
       }
       lk.lock();
       s->launch_ns += t_launched - t;
@@ -986,8 +989,13 @@ reset_status reset_server_create(const reset_server_config* cfg, reset_server** 
   uint64_t keep = UINT64_MAX;
   RST_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   s->slots.resize(c.streams);
+  // light batches run at the highest stream priority, heavy ones at the
+  // lowest, so blocks of light batches are scheduled first as SMs free up
+  int prio_lo = 0, prio_hi = 0;
+  RST_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   for (auto& sl : s->slots) {
-    RST_CUDA(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
+    RST_CUDA(cudaStreamCreateWithPriority(&sl.st, cudaStreamNonBlocking, prio_hi));
+    RST_CUDA(cudaStreamCreateWithPriority(&sl.st_lo, cudaStreamNonBlocking, prio_lo));
     RST_CUDA(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
   }
   try {
@@ -1131,10 +1139,11 @@ reset_status reset_server_destroy(reset_server* s) {
   if (s->worker.joinable()) s->worker.join();
   cudaError_t e = cudaSuccess;
   for (auto& sl : s->slots) {
-    if (sl.st) {
-      cudaError_t e2 = cudaStreamSynchronize(sl.st);
+    for (cudaStream_t* p : {&sl.st, &sl.st_lo}) {
+      if (!*p) continue;
+      cudaError_t e2 = cudaStreamSynchronize(*p);
       if (e == cudaSuccess) e = e2;
-      cudaStreamDestroy(sl.st);
+      cudaStreamDestroy(*p);
     }
     if (sl.ev) cudaEventDestroy(sl.ev);
     if (sl.arena) cudaFree(sl.arena);

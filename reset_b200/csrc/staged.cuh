@@ -17,7 +17,7 @@ constexpr int kOT = 512;                 // threads per CTA (2 CTAs, 32 warps pe
 constexpr int kOW = kOT / 32;            // warps per CTA
 constexpr int kCtaTab = 24576;           // ints of shared memory per CTA (96 KB)
 constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (3072 ints)
-constexpr int kCtaSeg = 512;             // probers per CTA work unit
+constexpr int kCtaSeg = 8192;            // probers per CTA work unit
 constexpr int kBigGroup = 256;           // groups above this are CTA work
 constexpr int kCtaWork = 32768;          // probes that make a smaller group CTA work
 constexpr int kDirSeg = 256;             // probers per direct work unit

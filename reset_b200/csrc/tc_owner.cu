@@ -140,7 +140,9 @@ __global__ void __launch_bounds__(kOT)
   classify_owners(desc, goff, ent, n, b, units, wlist, dlist, dunits, ctr);
 }
 
-template <bool HIER, int R>
+// OWN: every owner's hits are also added to owner_hits[owner] (per-graph
+// counts of a batch of disjoint graphs are sums over their vertex ranges).
+template <bool HIER, int R, bool OWN = false>
 __global__ void __launch_bounds__(kOT, 2)
     tc_owner_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
                     const int2* __restrict__ ent, const int32_t* __restrict__ cols, int64_t m,
@@ -148,7 +150,8 @@ __global__ void __launch_bounds__(kOT, 2)
                     const int32_t* __restrict__ dlist, const int2* __restrict__ dunits,
                     int32_t* __restrict__ ctr,
                     const int32_t* __restrict__ table, int64_t bn, int b, int lg_max,
-                    unsigned long long* __restrict__ count, int32_t* __restrict__ status) {
+                    unsigned long long* __restrict__ count,
+                    unsigned long long* __restrict__ owner_hits, int32_t* __restrict__ status) {
   extern __shared__ __align__(128) int sm[];
   __shared__ __align__(8) uint64_t s_bar[kOW + 1];
   __shared__ int s_item, s_next;
@@ -160,6 +163,13 @@ __global__ void __launch_bounds__(kOT, 2)
   unsigned long long hits = 0;
   uint32_t par_cta = 0, par_warp = 0;
   const int n_units = ctr[0], n_warp = ctr[1], n_direct = ctr[2], n_dunits = ctr[6];
+  // this warp's hits since h0 credited to owner w (warp-collective)
+  auto credit = [&](int w, unsigned long long h0) {
+    if (OWN) {
+      const unsigned long long d = warp_sum_u64(hits - h0);
+      if (lane == 0 && d) atomicAdd(owner_hits + w, d);
+    }
+  };
 
   // ---- CTA units: the whole CTA stages one table, warps share its probers
   for (;;) {
@@ -183,6 +193,7 @@ __global__ void __launch_bounds__(kOT, 2)
     }
     const int g0 = __ldg(goff + unit.x) + unit.y * kCtaSeg;
     const int g1 = min(__ldg(goff + unit.x + 1), g0 + kCtaSeg);
+    const unsigned long long h0 = hits;
     for (;;) {
       int g = 0;
       if (lane == 0) g = g0 + atomicAdd(&s_next, 32);
@@ -191,6 +202,7 @@ __global__ void __launch_bounds__(kOT, 2)
       hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, sm, lg, lg_max, b, status,
                                    s_qx[warp], s_qh[warp]);
     }
+    credit(unit.x, h0);
     __syncthreads();
   }
 
@@ -205,11 +217,13 @@ __global__ void __launch_bounds__(kOT, 2)
     const int4 dw = __ldg(desc + unit.x);
     const int g0 = __ldg(goff + unit.x) + unit.y * kDirSeg;
     const int g1 = min(__ldg(goff + unit.x + 1), g0 + kDirSeg);
+    const unsigned long long h0 = hits;
     for (int g = g0; g < g1; g += 32) {
       const int2 e = g + lane < g1 ? __ldg(ent + g + lane) : make_int2(0, 0);
       hits += flat_probe<HIER>(cols, m, table, e.y, e.x, desc_toff(dw), desc_lg(dw), lg_max,
                                bn, b, status, [](int) {});
     }
+    credit(unit.x, h0);
   }
 
   // ---- warp owners: each warp stages a table in its own region
@@ -232,9 +246,11 @@ __global__ void __launch_bounds__(kOT, 2)
       return;
     }
     const int g0 = __ldg(goff + w), g1 = __ldg(goff + w + 1);
+    const unsigned long long h0 = hits;
     for (int g = g0; g < g1; g += 32)
       hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, W, lg, lg_max, b, status,
                                    s_qx[warp], s_qh[warp]);
+    credit(w, h0);
   }
 
   // ---- direct owners: 32 owners per warp, their (owner, prober) pairs
@@ -245,10 +261,10 @@ __global__ void __launch_bounds__(kOT, 2)
     ci = __shfl_sync(kFull, ci, 0);
     const int64_t i = (int64_t)ci * 32 + lane;
     if ((int64_t)ci * 32 >= n_direct) break;
-    int g0 = 0, P = 0, lg = 3;
+    int g0 = 0, P = 0, lg = 3, w = 0;
     int64_t toff = 0;
     if (i < n_direct) {
-      const int w = __ldg(dlist + i);
+      w = __ldg(dlist + i);
       const int4 dw = __ldg(desc + w);
       g0 = __ldg(goff + w);
       P = __ldg(goff + w + 1) - g0;
@@ -257,6 +273,11 @@ __global__ void __launch_bounds__(kOT, 2)
     }
     int TP;
     const int Q = warp_excl_scan(P, &TP);
+    // OWN: the queue arrays (idle in this phase) hold, per pair lane, its
+    // owner lane (s_qh) and, per owner lane, its hits (s_qx)
+    int* pair_owner = s_qh[warp];
+    int* own_hits = s_qx[warp];
+    if (OWN) own_hits[lane] = 0;
     for (int base = 0; base < TP; base += 32) {
       const int f = base + lane;
       const int k = owner_lane(Q, f);
@@ -265,9 +286,19 @@ __global__ void __launch_bounds__(kOT, 2)
       const int klg = __shfl_sync(kFull, lg, k);
       const int64_t kt = __shfl_sync(kFull, toff, k);
       const int2 e = f < TP ? __ldg(ent + kg + (f - kq)) : make_int2(0, 0);
+      if (OWN) {
+        pair_owner[lane] = k;
+        __syncwarp();
+      }
       hits += flat_probe<HIER>(cols, m, table, e.y, e.x, kt, klg, lg_max, bn, b, status,
-                               [](int) {});
+                               [&](int kk) {
+                                 if (OWN) atomicAdd(own_hits + pair_owner[kk], 1);
+                               });
+      if (OWN) __syncwarp();
     }
+    if (OWN && i < n_direct && own_hits[lane])
+      atomicAdd(owner_hits + w, (unsigned long long)own_hits[lane]);
+    if (OWN) __syncwarp();
   }
   hits = warp_sum_u64(hits);
   if (lane == 0 && hits) atomicAdd(count, hits);
@@ -287,7 +318,8 @@ int grid_stride_blocks(int64_t items_per_block_unit, int cap) {
 reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* koff,
                       const int32_t* kcols, int64_t mk, const int32_t* eoff,
                       const int32_t* ecols, const int32_t* echunk_rows, int64_t me,
-                      unsigned long long* count, cudaStream_t st) {
+                      unsigned long long* count, cudaStream_t st,
+                      unsigned long long* owner_hits) {
   const int64_t n = t->n;
   const int64_t m = me;
   if (n == 0 || me == 0 || mk == 0) return RESET_OK;
@@ -345,24 +377,28 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   }
   if (e == cudaSuccess) {
     const size_t smem = sizeof(int) * kCtaTab;
-    const void* k = t->hier ? (const void*)tc_owner_kernel<true, 4>
-                            : (const void*)tc_owner_kernel<false, 4>;
+    const bool own = owner_hits != nullptr;
+#define OWN_K(H, O) tc_owner_kernel<H, 4, O>
+    const void* k = t->hier ? (own ? (const void*)OWN_K(true, true) : (const void*)OWN_K(true, false))
+                            : (own ? (const void*)OWN_K(false, true)
+                                   : (const void*)OWN_K(false, false));
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kOT, smem);
     if (e == cudaSuccess) {
       const int grid = sms * (per_sm > 0 ? per_sm : 1);
       note_launch();
-      if (t->hier)
-        tc_owner_kernel<true, 4><<<grid, kOT, smem, st>>>(
-            kdesc, goff, ent, kcols, mk, units, wlist, dlist, dunits, ctr, t->d_table,
-            t->bucket_num,
-            t->bucket, t->lg_max, count, t->d_status);
-      else
-        tc_owner_kernel<false, 4><<<grid, kOT, smem, st>>>(
-            kdesc, goff, ent, kcols, mk, units, wlist, dlist, dunits, ctr, t->d_table,
-            t->bucket_num,
-            t->bucket, t->lg_max, count, t->d_status);
+#define OWN_LAUNCH(H, O)                                                                   \
+  OWN_K(H, O)<<<grid, kOT, smem, st>>>(kdesc, goff, ent, kcols, mk, units, wlist, dlist,    \
+                                       dunits, ctr, t->d_table, t->bucket_num, t->bucket,  \
+                                       t->lg_max, count, owner_hits, t->d_status)
+      if (t->hier) {
+        if (own) OWN_LAUNCH(true, true); else OWN_LAUNCH(true, false);
+      } else {
+        if (own) OWN_LAUNCH(false, true); else OWN_LAUNCH(false, false);
+      }
+#undef OWN_LAUNCH
+#undef OWN_K
       e = cudaGetLastError();
     }
   }
@@ -372,3 +408,43 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
 }
 
 }  // namespace rst
+
+using namespace rst;
+
+extern "C" reset_status reset_tc_count_batch(const reset_table* t, const int32_t* d_off,
+                                             const int32_t* d_cols, int64_t m,
+                                             const int32_t* d_graph_off, int32_t n_graphs,
+                                             uint64_t* d_counts, reset_stream_t stream) {
+  if (!t || !d_counts || !d_graph_off) return arg_fail("NULL table, graph offsets or counts");
+  if (n_graphs < 1) return arg_fail("n_graphs must be >= 1");
+  if (m < 0 || m > INT32_MAX - 4) return arg_fail("m out of range");
+  if (m > 0 && (!d_cols || !d_off)) return arg_fail("NULL offsets or cols");
+  if ((reinterpret_cast<uintptr_t>(d_cols) & 15) != 0)
+    return arg_fail("reset_tc_count_batch needs a 16-byte aligned column array");
+  if (d_off != t->build_off || m != t->m)
+    return arg_fail("d_off/m must be the CSR the table was built on");
+  cudaStream_t st = as_stream(stream);
+  RST_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(uint64_t) * (size_t)n_graphs, st));
+  if (m == 0 || t->n == 0) return RESET_OK;
+  size_t cub_bytes = 0;
+  RST_CUDA(cub::DeviceSegmentedReduce::Sum(nullptr, cub_bytes, (unsigned long long*)nullptr,
+                                           (unsigned long long*)nullptr, n_graphs, d_graph_off,
+                                           d_graph_off + 1, st));
+  const size_t own_bytes = (sizeof(unsigned long long) * ((size_t)t->n + 1) + 255) & ~(size_t)255;
+  char* buf = nullptr;
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&buf), own_bytes + 256 + cub_bytes, st));
+  auto* owner_hits = reinterpret_cast<unsigned long long*>(buf);
+  auto* total = reinterpret_cast<unsigned long long*>(buf + own_bytes);
+  cudaError_t e = cudaMemsetAsync(buf, 0, own_bytes + 256, st);
+  reset_status s = RESET_OK;
+  if (e == cudaSuccess)
+    s = tc_owner(t, t->d_desc, d_off, d_cols, m, d_off, d_cols, t->d_chunk_row, m, total, st,
+                 owner_hits);
+  if (e == cudaSuccess && s == RESET_OK)
+    e = cub::DeviceSegmentedReduce::Sum(buf + own_bytes + 256, cub_bytes, owner_hits,
+                                        reinterpret_cast<unsigned long long*>(d_counts), n_graphs,
+                                        d_graph_off, d_graph_off + 1, st);
+  cudaFreeAsync(buf, st);
+  if (e != cudaSuccess) return cuda_fail(e, "reset_tc_count_batch", __FILE__, __LINE__);
+  return s;
+}

@@ -487,3 +487,74 @@ def test_clique4_complete_graph(R, cuda):
     d_off, d_cols = dev(off, torch), dev(cols, torch)
     t = R.Table(d_off, d_cols)
     assert R.clique4_count(t, d_off, d_cols) == comb(n, 4)
+
+
+@pytest.mark.parametrize("scale,hier", [(10, True), (12, False), (13, True)])
+def test_clique_k_matches_oracle(R, cuda, oracle_mod, scale, hier):
+    """k-cliques (SMOG's clique search over hash probes) equal the oracle's
+    depth-first merge restatement for k = 3..7; k = 3 and 4 also equal the
+    triangle and 4-clique counts."""
+    torch = cuda
+    off, cols = oracle_mod.rmat_graph(scale, 16, 0x5EED0500 + scale, oriented=True)
+    d_off, d_cols = dev(off, torch), dev(cols, torch)
+    t = R.Table(d_off, d_cols, hierarchical=hier)
+    for k in range(3, 8):
+        assert R.clique_count(t, d_off, d_cols, k) == oracle_mod.clique_k(off, cols, k), k
+    assert R.clique_count(t, d_off, d_cols, 3) == oracle_mod.tc_merge(off, cols)
+    assert R.clique_count(t, d_off, d_cols, 4) == R.clique4_count(t, d_off, d_cols)
+    t.check()
+
+
+def test_clique_k_complete_graph_and_limits(R, cuda):
+    torch = cuda
+    from math import comb
+    from reset_b200._lib import ResetError
+    n = 24
+    rows = [list(range(u + 1, n)) for u in range(n)]
+    off = np.zeros(n + 1, np.int32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    cols = np.array(sum(rows, []), np.int32)
+    d_off, d_cols = dev(off, torch), dev(cols, torch)
+    t = R.Table(d_off, d_cols)
+    for k in (3, 5, 9, 16):
+        assert R.clique_count(t, d_off, d_cols, k) == comb(n, k), k
+    for k in (2, 17):
+        with pytest.raises(ResetError):
+            R.clique_count(t, d_off, d_cols, k)
+
+
+def block_diagonal(graphs):
+    """Disjoint oriented graphs [(off, cols)] -> one CSR + vertex offsets."""
+    offs, colss, gro = [np.zeros(1, np.int64)], [], [0]
+    vbase = ebase = 0
+    for off, cols in graphs:
+        offs.append(off[1:].astype(np.int64) + ebase)
+        colss.append(cols.astype(np.int64) + vbase)
+        vbase += off.size - 1
+        ebase += cols.size
+        gro.append(vbase)
+    return (np.concatenate(offs).astype(np.int32), np.concatenate(colss).astype(np.int32),
+            np.array(gro, np.int32))
+
+
+@pytest.mark.parametrize("hier", [True, False])
+def test_tc_count_batch_per_graph(R, cuda, oracle_mod, hier):
+    """One owner-grouped count over a batch of disjoint graphs of different
+    sizes (including empty and edgeless ones) gives every graph's own
+    triangle count, as the oracle counts them one by one."""
+    torch = cuda
+    graphs = []
+    for i, scale in enumerate([6, 9, 1, 11, 8, 7, 10, 5]):
+        if i == 2:
+            graphs.append((np.zeros(4, np.int32), np.zeros(0, np.int32)))  # edgeless
+            continue
+        graphs.append(oracle_mod.rmat_graph(scale, 16, 0x5EED0600 + i, oriented=True))
+    off, cols, gro = block_diagonal(graphs)
+    want = [oracle_mod.tc_merge(o, c) if c.size else 0 for o, c in graphs]
+    d_off, d_cols, d_gro = dev(off, torch), dev(cols, torch), dev(gro, torch)
+    t = R.Table(d_off, d_cols, hierarchical=hier, hash_order=True)
+    for c in (d_cols, t.hash_order):
+        got = host(R.tc_count_batch(t, d_off, c, d_gro)).tolist()
+        assert got == want
+    assert R.tc_count(t, d_off, t.hash_order) == sum(want)
+    t.check()

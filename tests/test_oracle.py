@@ -300,3 +300,40 @@ def test_tc_counts_fixture_pins_small_scales(oracle_mod):
         assert oracle_mod.tc_merge(off, cols) == c["triangles"]
     for s in ("20", "22", "24"):
         assert rec["counts"][s]["triangles"] > 0
+
+
+def test_clique_k_oracle_against_brute_force(oracle_mod):
+    from math import comb
+    for n in (3, 6, 9):
+        rows = [list(range(u + 1, n)) for u in range(n)]
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum([len(r) for r in rows])
+        cols = np.array(sum(rows, []), np.int32)
+        for k in range(3, 8):
+            assert oracle_mod.clique_k(off, cols, k) == comb(n, k)
+    off, cols = oracle_mod.rmat_graph(7, 8, 3, oriented=True)
+    n = off.size - 1
+    und = [set() for _ in range(n)]
+    for u in range(n):
+        for v in cols[off[u]:off[u + 1]].tolist():
+            und[u].add(v)
+            und[v].add(u)
+
+    def count(k):
+        total = 0
+
+        def ext(last, cand, left):
+            nonlocal total
+            if left == 0:
+                total += 1
+                return
+            for w in cand:
+                if w > last:
+                    ext(w, cand & und[w], left - 1)
+        for u in range(n):
+            ext(u, und[u], k - 1)
+        return total
+    for k in (3, 4, 5, 6):
+        assert oracle_mod.clique_k(off, cols, k) == count(k)
+    assert oracle_mod.clique_k(off, cols, 3) == oracle_mod.tc_merge(off, cols)
+    assert oracle_mod.clique_k(off, cols, 4) == oracle_mod.clique4(off, cols)
