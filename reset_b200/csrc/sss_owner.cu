@@ -180,7 +180,8 @@ __global__ void __launch_bounds__(kOT, 2)
     const int4 dw = __ldg(desc + unit.x);
     const int lg = desc_lg(dw);
     if (tid == 0) stage_table(sm, table, desc_toff(dw), lg, bn, b, &s_bar[kOW]);
-    const bool ok = __syncthreads_and(mbar_wait(&s_bar[kOW], par_cta));
+    const bool ok =
+        __syncthreads_and(stage_wait(&s_bar[kOW], par_cta, sm, lg, b, tid == 0));
     par_cta ^= 1u;
     if (!ok) {
       if (tid == 0) atomicOr(status, kErrStageTimeout);
@@ -191,10 +192,10 @@ __global__ void __launch_bounds__(kOT, 2)
     const int g1 = min(__ldg(goff + unit.x + 1), g0 + kCtaSeg);
     for (;;) {
       int g = 0;
-      if (lane == 0) g = g0 + atomicAdd(&s_next, 32);
+      if (lane == 0) g = g0 + atomicAdd(&s_next, kGrab);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      batch(g, min(32, g1 - g), sm, lg, dw.y);
+      batch(g, min(kGrab, g1 - g), sm, lg, dw.y);
     }
     __syncthreads();
   }
@@ -236,7 +237,8 @@ __global__ void __launch_bounds__(kOT, 2)
     const int lg = desc_lg(dw);
     __syncwarp();
     if (lane == 0) stage_table(W, table, desc_toff(dw), lg, bn, b, &s_bar[warp]);
-    const bool ok = __all_sync(kFull, mbar_wait(&s_bar[warp], par_warp));
+    const bool ok = __all_sync(kFull, stage_wait(&s_bar[warp], par_warp, W, lg, b, lane == 0));
+    __syncwarp();
     par_warp ^= 1u;
     if (!ok) {
       if (lane == 0) atomicOr(status, kErrStageTimeout);

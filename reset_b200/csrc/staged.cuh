@@ -16,8 +16,14 @@ constexpr int kWaitLimit = 1 << 22;  // polls of a bulk-copy barrier before givi
 constexpr int kOT = 512;                 // threads per CTA (2 CTAs, 32 warps per SM)
 constexpr int kOW = kOT / 32;            // warps per CTA
 constexpr int kCtaTab = 24576;           // ints of shared memory per CTA (96 KB)
-constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (3072 ints)
+constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (1536 ints)
 constexpr int kCtaSeg = 8192;            // probers per CTA work unit
+// Probers a warp takes at a time from a CTA unit.  A unit averages a few
+// hundred probers of ~100-300 keys each; taking 32 at a time left 16 warps
+// with one or two uneven batches, so the CTA waited ~1/3 of each unit at
+// its closing barrier (modelled on the scale-20 groups: 65% balance at 32,
+// 92% at 8).  Each batch still flattens its rows' keys across the lanes.
+constexpr int kGrab = 8;
 constexpr int kBigGroup = 256;           // groups above this are CTA work
 constexpr int kCtaWork = 32768;          // probes that make a smaller group CTA work
 constexpr int kDirSeg = 256;             // probers per direct work unit
@@ -171,24 +177,54 @@ __device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h,
 
 constexpr int kQueue = 128;  // pending probes a warp queues per round (32 lanes x 4 keys)
 
-// The keys of up to 32 probing rows (lane i: ent[i] = {row start, row
-// length} in cols) looked up in one staged table.  The rows' 16-byte chunks
-// are flattened across the lanes (round r: lane i loads chunk 32r+i of the
-// concatenation, its row found by a shuffle binary search) and R rounds are
-// in flight at once.  Every key's first two probe slots (slots 0 and 1 of
-// its home bucket; with one slot per bucket, the home and next bucket) are
-// read and resolved without branching; probes that both slots leave open are
-// queued in this warp's shared-memory queue (qx, qh: kQueue entries each)
-// and walked by all lanes together, so the rare long walks do not idle the
-// warp.  Returns this lane's hits; with PAIRS, the hits of row i are also
-// added to s_cnt[i] (32 shared-memory counters of this warp, zeroed by the
-// caller).
-template <bool HIER, int R, bool PAIRS = false>
+// Waits (bounded) for a staged table; with one slot per bucket the writer
+// then appends a copy of bucket 0 after the last bucket (S[L] = S[0]), so
+// the home bucket's successor is S[h + 1] without a wrap.  A table staged
+// with b = 1 is a power of two no larger than half its region (kCtaTab,
+// kWarpTab are 3 * 2^k), so S[L] lies inside the region.  The caller's
+// barrier publishes the copy.
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, int* S, int lg, int b,
+                                           bool writer) {
+  const bool ok = mbar_wait(bar, parity);
+  if (ok && writer && b == 1) S[1 << lg] = S[0];
+  return ok;
+}
+
+// Largest lane k < NR with P_k <= f (P nondecreasing across lanes, P_0 = 0;
+// every row at or past NR is empty).
+template <int NR>
+__device__ __forceinline__ int owner_lane_n(int P, int f) {
+  int k = 0;
+#pragma unroll
+  for (int step = NR / 2; step >= 1; step >>= 1) {
+    const int pk = __shfl_sync(kFull, P, k + step);
+    if (pk <= f) k += step;
+  }
+  return k;
+}
+
+// The keys of up to NR probing rows (NR a power of two <= 32; lane i:
+// ent[i] = {row start, row length} in cols) looked up in one staged table
+// (plane k at S + k*L; with b = 1 padded by stage_wait).  The rows' 16-byte
+// chunks are flattened across the lanes (round r: lane i loads chunk 32r+i
+// of the concatenation, its row found by a shuffle binary search over the NR
+// rows) and R rounds are in flight at once.  Elements of a chunk outside its
+// row become the sentinel -2, which matches no slot (keys are >= 0, empty
+// slots -1), so every element is probed without a validity test.  Every
+// key's first two probe slots (slots 0 and 1 of its home bucket; with one
+// slot per bucket, the home and next bucket) are read and resolved without
+// branching; probes that both slots leave open are queued in this warp's
+// shared-memory queue (qx, qh: kQueue entries each) and walked by all lanes
+// together, so the rare long walks do not idle the warp.  Returns this
+// lane's hits; with PAIRS, the hits of row i are also added to s_cnt[i] (32
+// shared-memory counters of this warp, zeroed by the caller).
+template <bool HIER, int R, bool PAIRS = false, int NR = 32>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
                                                 int32_t* status, int* qx, int* qh,
                                                 int* s_cnt = nullptr) {
+  static_assert(NR >= 1 && NR <= 32 && (NR & (NR - 1)) == 0, "NR: a power of two <= 32");
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
@@ -199,25 +235,25 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   const int L = 1 << lg;
   const unsigned hmask = HIER ? ((1u << lg_max) - 1u) : (unsigned)(L - 1);
   const int hsh = HIER ? (lg_max - lg) : 0;
-  // the second probe slot and where a queued walk continues
-  const int off1 = b > 1 ? L : 0;   // slot 1 of the home bucket, or ...
-  const int inc1 = b > 1 ? 0 : 1;   // ... slot 0 of the next bucket
-  const int kcont = b > 1 ? 2 : 1;  // the slot of bucket h1 a queued walk continues at
+  // the second probe slot: slot 1 of the home bucket, or (b = 1) the next
+  // bucket, S[h + 1] in the padded copy; a queued walk continues from slot
+  // kcont of bucket h + inc1
+  const int off1 = b > 1 ? L : 1;
+  const int inc1 = b > 1 ? 0 : 1;
+  const int kcont = b > 1 ? 2 : 1;
   const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
   const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
   unsigned hits = 0;
   for (int base = 0; base < total; base += 32 * R) {
     int x[R][4];
-    unsigned vm[R];  // bit j: element j of this lane's chunk belongs to the row
-    int kk[R];       // the row (lane index) of this lane's chunk, -1 if none
+    int kk[R];  // the row (lane index) of this lane's chunk, -1 if none
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      vm[r] = 0;
       kk[r] = -1;
-      x[r][0] = x[r][1] = x[r][2] = x[r][3] = 0;
+      x[r][0] = x[r][1] = x[r][2] = x[r][3] = -2;
       if (base + r * 32 < total) {  // warp-uniform
         const int f = base + r * 32 + lane;
-        const int k = owner_lane(P, f);
+        const int k = owner_lane_n<NR>(P, f);
         const int kp = __shfl_sync(kFull, P, k);
         const int kb = __shfl_sync(kFull, e.x, k);
         const int kd = __shfl_sync(kFull, e.y, k);
@@ -226,9 +262,8 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
           // m <= 2^31 - 5 (checked on the host): 4c + 3 fits an int
           const int c = (kb >> 2) + (f - kp);
           const int i0 = c * 4;
-          const int lo = max(kb - i0, 0);
-          const int hi = min(kb + kd - i0, 4);
-          vm[r] = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+          const int lo = kb - i0;       // elements j < lo precede the row
+          const int hi = kb + kd - i0;  // elements j >= hi follow it
           if (c < full4) {
             const int4 q = __ldg(cols4 + c);
             x[r][0] = q.x;
@@ -238,7 +273,12 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
           } else {
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-              if ((vm[r] >> j) & 1u) x[r][j] = __ldg(cols + i0 + j);
+              if (j >= lo && j < hi) x[r][j] = __ldg(cols + i0 + j);
+          }
+          if (lo > 0 || hi < 4) {  // the first or last chunk of its row
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (j < lo || j >= hi) x[r][j] = -2;
           }
         }
       }
@@ -250,21 +290,18 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
       int nq = 0;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const bool act = (vm[r] >> j) & 1u;
         const int xx = x[r][j];
         const int h = (int)(((unsigned)xx & hmask) >> hsh);
-        const int h1 = (h + inc1) & (L - 1);
-        const int s0 = act ? S[h] : -1;
-        const int s1 = act ? S[off1 + h1] : -1;
-        const bool m0 = s0 == xx, e0 = s0 == -1, m1 = s1 == xx, e1 = s1 == -1;
-        hr += (unsigned)(act & (m0 | (!e0 & m1)));
-        const bool pend = act & !m0 & !e0 & !m1 & !e1;
+        const int s0 = S[h];
+        const int s1 = S[h + off1];
+        hr += (unsigned)((s0 == xx) | ((s0 != -1) & (s1 == xx)));
+        const bool pend = (s0 != xx) & (s0 != -1) & (s1 != xx) & (s1 != -1);
         const unsigned pm = __ballot_sync(kFull, pend);
         if (pend) {
           // continue at slot 2 of the home bucket (or, one slot per bucket,
-          // at the bucket after h1); the row rides along for PAIRS
+          // at the bucket after h + 1); the row rides along for PAIRS
           qx[nq + __popc(pm & lt)] = xx;
-          qh[nq + __popc(pm & lt)] = (h1 << 10) | (kcont << 5) | kk[r];
+          qh[nq + __popc(pm & lt)] = ((h + inc1) << 10) | (kcont << 5) | (kk[r] & 31);
         }
         nq += __popc(pm);
       }

@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(kOT, 2)
     const int4 dw = __ldg(desc + unit.x);
     const int lg = desc_lg(dw);
     if (tid == 0) stage_table(sm, table, desc_toff(dw), lg, bn, b, &s_bar[kOW]);
-    const bool ok = __syncthreads_and(mbar_wait(&s_bar[kOW], par_cta));
+    const bool ok =
+        __syncthreads_and(stage_wait(&s_bar[kOW], par_cta, sm, lg, b, tid == 0));
     par_cta ^= 1u;
     if (!ok) {  // a copy that never landed: report, let it drain, stop
       if (tid == 0) atomicOr(status, kErrStageTimeout);
@@ -196,11 +197,11 @@ __global__ void __launch_bounds__(kOT, 2)
     const unsigned long long h0 = hits;
     for (;;) {
       int g = 0;
-      if (lane == 0) g = g0 + atomicAdd(&s_next, 32);
+      if (lane == 0) g = g0 + atomicAdd(&s_next, kGrab);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, sm, lg, lg_max, b, status,
-                                   s_qx[warp], s_qh[warp]);
+      hits += staged_keys<HIER, R, false, kGrab>(ent + g, min(kGrab, g1 - g), cols, m, sm, lg,
+                                                 lg_max, b, status, s_qx[warp], s_qh[warp]);
     }
     credit(unit.x, h0);
     __syncthreads();
@@ -238,7 +239,8 @@ __global__ void __launch_bounds__(kOT, 2)
     const int lg = desc_lg(dw);
     __syncwarp();
     if (lane == 0) stage_table(W, table, desc_toff(dw), lg, bn, b, &s_bar[warp]);
-    const bool ok = __all_sync(kFull, mbar_wait(&s_bar[warp], par_warp));
+    const bool ok = __all_sync(kFull, stage_wait(&s_bar[warp], par_warp, W, lg, b, lane == 0));
+    __syncwarp();
     par_warp ^= 1u;
     if (!ok) {
       if (lane == 0) atomicOr(status, kErrStageTimeout);
