@@ -15,8 +15,11 @@ constexpr int kWaitLimit = 1 << 22;  // polls of a bulk-copy barrier before givi
 // Launch shape and bins of the owner-grouped kernels.
 constexpr int kOT = 512;                 // threads per CTA (2 CTAs, 32 warps per SM)
 constexpr int kOW = kOT / 32;            // warps per CTA
-constexpr int kCtaTab = 24576;           // ints of shared memory per CTA (96 KB)
-constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (1536 ints)
+// Ints of shared memory per CTA for staged tables (80 KB): every power-of-two
+// plane size with b = 1, 2, 4 or 5 slots that 96 KB held still fits, and the
+// 16 KB saved doubles the pending-probe queues of the triangle count.
+constexpr int kCtaTab = 20480;
+constexpr int kWarpTab = kCtaTab / kOW;  // a warp's region (1280 ints)
 constexpr int kCtaSeg = 8192;            // probers per CTA work unit
 // Probers a warp takes at a time from a CTA unit.  A unit averages a few
 // hundred probers of ~100-300 keys each; taking 32 at a time left 16 warps
@@ -175,14 +178,15 @@ __device__ __forceinline__ unsigned smem_walk(int x, const int* S, int L, int h,
   return 0;
 }
 
-constexpr int kQueue = 128;  // pending probes a warp queues per round (32 lanes x 4 keys)
+// Pending probes one round of 32 lanes x 4 keys can queue.
+constexpr int kQueue = 128;
 
 // Waits (bounded) for a staged table; with one slot per bucket the writer
 // then appends a copy of bucket 0 after the last bucket (S[L] = S[0]), so
-// the home bucket's successor is S[h + 1] without a wrap.  A table staged
-// with b = 1 is a power of two no larger than half its region (kCtaTab,
-// kWarpTab are 3 * 2^k), so S[L] lies inside the region.  The caller's
-// barrier publishes the copy.
+// the home bucket's successor is S[h + 1] without a wrap.  Neither region
+// size (kCtaTab, kWarpTab) is a power of two, so a staged b = 1 table (a
+// power of two) ends strictly inside its region and S[L] is in it too.  The
+// caller's barrier publishes the copy.
 __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, int* S, int lg, int b,
                                            bool writer) {
   const bool ok = mbar_wait(bar, parity);
@@ -214,17 +218,20 @@ __device__ __forceinline__ int owner_lane_n(int P, int f) {
 // key's first two probe slots (slots 0 and 1 of its home bucket; with one
 // slot per bucket, the home and next bucket) are read and resolved without
 // branching; probes that both slots leave open are queued in this warp's
-// shared-memory queue (qx, qh: kQueue entries each) and walked by all lanes
-// together, so the rare long walks do not idle the warp.  Returns this
-// lane's hits; with PAIRS, the hits of row i are also added to s_cnt[i] (32
-// shared-memory counters of this warp, zeroed by the caller).
-template <bool HIER, int R, bool PAIRS = false, int NR = 32>
+// shared-memory queue (qx, qh: QCAP entries each, QCAP >= kQueue) and walked
+// by all lanes together once more than QCAP - kQueue are pending (and before
+// returning), so the rare long walks neither idle the warp nor run with few
+// lanes.  Returns this lane's hits; with PAIRS, the hits of row i are also
+// added to s_cnt[i] (32 shared-memory counters of this warp, zeroed by the
+// caller).
+template <bool HIER, int R, bool PAIRS = false, int NR = 32, int QCAP = kQueue>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
                                                 int32_t* status, int* qx, int* qh,
                                                 int* s_cnt = nullptr) {
   static_assert(NR >= 1 && NR <= 32 && (NR & (NR - 1)) == 0, "NR: a power of two <= 32");
+  static_assert(QCAP >= kQueue, "the queue must hold one round");
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
@@ -244,6 +251,21 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
   const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
   unsigned hits = 0;
+  int nq = 0;  // queued probes (warp-uniform)
+  auto walk_queue = [&]() {
+    __syncwarp();
+    for (int i = lane; i < nq; i += 32) {
+      const int v = qh[i];
+      const unsigned hit = smem_walk(qx[i], S, L, v >> 10, (v >> 5) & 31, b, status);
+      if (PAIRS) {
+        if (hit) atomicAdd(s_cnt + (v & 31), 1);
+      } else {
+        hits += hit;
+      }
+    }
+    __syncwarp();
+    nq = 0;
+  };
   for (int base = 0; base < total; base += 32 * R) {
     int x[R][4];
     int kk[R];  // the row (lane index) of this lane's chunk, -1 if none
@@ -287,7 +309,6 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
     for (int r = 0; r < R; ++r) {
       if (base + r * 32 >= total) break;  // warp-uniform
       unsigned hr = 0;
-      int nq = 0;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int xx = x[r][j];
@@ -305,19 +326,7 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         }
         nq += __popc(pm);
       }
-      if (nq) {
-        __syncwarp();
-        for (int i = lane; i < nq; i += 32) {
-          const int v = qh[i];
-          const unsigned hit = smem_walk(qx[i], S, L, v >> 10, (v >> 5) & 31, b, status);
-          if (PAIRS) {
-            if (hit) atomicAdd(s_cnt + (v & 31), 1);
-          } else {
-            hits += hit;
-          }
-        }
-        __syncwarp();
-      }
+      if (nq > QCAP - kQueue) walk_queue();
       hits += hr;
       if (PAIRS) {
         const unsigned grp = __match_any_sync(kFull, kk[r]);
@@ -326,6 +335,7 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
       }
     }
   }
+  if (nq) walk_queue();
   return hits;
 }
 

@@ -155,7 +155,10 @@ __global__ void __launch_bounds__(kOT, 2)
   extern __shared__ __align__(128) int sm[];
   __shared__ __align__(8) uint64_t s_bar[kOW + 1];
   __shared__ int s_item, s_next;
-  __shared__ int s_qx[kOW][kQueue], s_qh[kOW][kQueue];
+  // pending-probe queues of two rounds: walked once at least one round's
+  // worth is queued, so the walks run with (nearly) full warps
+  constexpr int QCAP = 2 * kQueue;
+  __shared__ int s_qx[kOW][QCAP], s_qh[kOW][QCAP];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= kOW) mbar_init(&s_bar[tid]);
   fence_mbar_init();
@@ -200,8 +203,9 @@ __global__ void __launch_bounds__(kOT, 2)
       if (lane == 0) g = g0 + atomicAdd(&s_next, kGrab);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      hits += staged_keys<HIER, R, false, kGrab>(ent + g, min(kGrab, g1 - g), cols, m, sm, lg,
-                                                 lg_max, b, status, s_qx[warp], s_qh[warp]);
+      hits += staged_keys<HIER, R, false, kGrab, QCAP>(ent + g, min(kGrab, g1 - g), cols, m,
+                                                       sm, lg, lg_max, b, status, s_qx[warp],
+                                                       s_qh[warp]);
     }
     credit(unit.x, h0);
     __syncthreads();
@@ -250,8 +254,8 @@ __global__ void __launch_bounds__(kOT, 2)
     const int g0 = __ldg(goff + w), g1 = __ldg(goff + w + 1);
     const unsigned long long h0 = hits;
     for (int g = g0; g < g1; g += 32)
-      hits += staged_keys<HIER, R>(ent + g, min(32, g1 - g), cols, m, W, lg, lg_max, b, status,
-                                   s_qx[warp], s_qh[warp]);
+      hits += staged_keys<HIER, R, false, 32, QCAP>(ent + g, min(32, g1 - g), cols, m, W, lg,
+                                                    lg_max, b, status, s_qx[warp], s_qh[warp]);
     credit(w, h0);
   }
 
