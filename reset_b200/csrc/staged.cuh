@@ -194,6 +194,30 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, int* 
   return ok;
 }
 
+// Walks queued keys q[0, nq) of one staged table (all lanes, nq
+// warp-uniform): each key's first two probe slots held other keys, so its
+// walk resumes after them -- slot 2 of its home bucket, or with one slot per
+// bucket the bucket after the next.  Returns this lane's hits.
+template <bool HIER>
+__device__ __forceinline__ unsigned walk_keys(const int* q, int nq, const int* S, int lg,
+                                              int lg_max, int b, int32_t* status) {
+  const int lane = threadIdx.x & 31;
+  const int L = 1 << lg;
+  const unsigned hmask = HIER ? ((1u << lg_max) - 1u) : (unsigned)(L - 1);
+  const int hsh = HIER ? (lg_max - lg) : 0;
+  const int inc1 = b > 1 ? 0 : 1;
+  const int kcont = b > 1 ? 2 : 1;
+  unsigned hits = 0;
+  __syncwarp();
+  for (int i = lane; i < nq; i += 32) {
+    const int x = q[i];
+    const int h = (int)(((unsigned)x & hmask) >> hsh);
+    hits += smem_walk(x, S, L, h + inc1, kcont, b, status);
+  }
+  __syncwarp();
+  return hits;
+}
+
 // Largest lane k < NR with P_k <= f (P nondecreasing across lanes, P_0 = 0;
 // every row at or past NR is empty).
 template <int NR>
@@ -224,14 +248,21 @@ __device__ __forceinline__ int owner_lane_n(int P, int f) {
 // lanes.  Returns this lane's hits; with PAIRS, the hits of row i are also
 // added to s_cnt[i] (32 shared-memory counters of this warp, zeroed by the
 // caller).
-template <bool HIER, int R, bool PAIRS = false, int NR = 32, int QCAP = kQueue>
+//
+// KEEP (counting only): the queue holds keys alone (their walk restarts from
+// the hash) and outlives the call: *nq_keep carries its length from call to
+// call over one staged table, and the caller walks the rest with walk_keys
+// before the table changes.
+template <bool HIER, int R, bool PAIRS = false, int NR = 32, int QCAP = kQueue,
+          bool KEEP = false>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
                                                 int32_t* status, int* qx, int* qh,
-                                                int* s_cnt = nullptr) {
+                                                int* s_cnt = nullptr, int* nq_keep = nullptr) {
   static_assert(NR >= 1 && NR <= 32 && (NR & (NR - 1)) == 0, "NR: a power of two <= 32");
   static_assert(QCAP >= kQueue, "the queue must hold one round");
+  static_assert(!(KEEP && PAIRS), "a kept queue carries no rows");
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
@@ -251,8 +282,13 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
   const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
   unsigned hits = 0;
-  int nq = 0;  // queued probes (warp-uniform)
+  int nq = KEEP ? *nq_keep : 0;  // queued probes (warp-uniform)
   auto walk_queue = [&]() {
+    if (KEEP) {
+      hits += walk_keys<HIER>(qx, nq, S, lg, lg_max, b, status);
+      nq = 0;
+      return;
+    }
     __syncwarp();
     for (int i = lane; i < nq; i += 32) {
       const int v = qh[i];
@@ -321,8 +357,9 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         if (pend) {
           // continue at slot 2 of the home bucket (or, one slot per bucket,
           // at the bucket after h + 1); the row rides along for PAIRS
-          qx[nq + __popc(pm & lt)] = xx;
-          qh[nq + __popc(pm & lt)] = ((h + inc1) << 10) | (kcont << 5) | (kk[r] & 31);
+          const int pos = nq + __popc(pm & lt);
+          qx[pos] = xx;
+          if (!KEEP) qh[pos] = ((h + inc1) << 10) | (kcont << 5) | (kk[r] & 31);
         }
         nq += __popc(pm);
       }
@@ -335,7 +372,10 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
       }
     }
   }
-  if (nq) walk_queue();
+  if (KEEP)
+    *nq_keep = nq;
+  else if (nq)
+    walk_queue();
   return hits;
 }
 

@@ -155,10 +155,11 @@ __global__ void __launch_bounds__(kOT, 2)
   extern __shared__ __align__(128) int sm[];
   __shared__ __align__(8) uint64_t s_bar[kOW + 1];
   __shared__ int s_item, s_next;
-  // pending-probe queues of two rounds: walked once at least one round's
-  // worth is queued, so the walks run with (nearly) full warps
-  constexpr int QCAP = 2 * kQueue;
-  __shared__ int s_qx[kOW][QCAP], s_qh[kOW][QCAP];
+  // pending-probe queues (keys only) of four rounds, kept over all the
+  // batches a warp takes from one staged table and walked once three rounds'
+  // worth is queued (or the table changes), so walks run with full warps
+  constexpr int QCAP = 4 * kQueue;
+  __shared__ int s_q[kOW][QCAP];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= kOW) mbar_init(&s_bar[tid]);
   fence_mbar_init();
@@ -198,15 +199,17 @@ __global__ void __launch_bounds__(kOT, 2)
     const int g0 = __ldg(goff + unit.x) + unit.y * kCtaSeg;
     const int g1 = min(__ldg(goff + unit.x + 1), g0 + kCtaSeg);
     const unsigned long long h0 = hits;
+    int nq = 0;
     for (;;) {
       int g = 0;
       if (lane == 0) g = g0 + atomicAdd(&s_next, kGrab);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      hits += staged_keys<HIER, R, false, kGrab, QCAP>(ent + g, min(kGrab, g1 - g), cols, m,
-                                                       sm, lg, lg_max, b, status, s_qx[warp],
-                                                       s_qh[warp]);
+      hits += staged_keys<HIER, R, false, kGrab, QCAP, true>(
+          ent + g, min(kGrab, g1 - g), cols, m, sm, lg, lg_max, b, status, s_q[warp], nullptr,
+          nullptr, &nq);
     }
+    if (nq) hits += walk_keys<HIER>(s_q[warp], nq, sm, lg, lg_max, b, status);
     credit(unit.x, h0);
     __syncthreads();
   }
@@ -253,9 +256,12 @@ __global__ void __launch_bounds__(kOT, 2)
     }
     const int g0 = __ldg(goff + w), g1 = __ldg(goff + w + 1);
     const unsigned long long h0 = hits;
+    int nq = 0;
     for (int g = g0; g < g1; g += 32)
-      hits += staged_keys<HIER, R, false, 32, QCAP>(ent + g, min(32, g1 - g), cols, m, W, lg,
-                                                    lg_max, b, status, s_qx[warp], s_qh[warp]);
+      hits += staged_keys<HIER, R, false, 32, QCAP, true>(ent + g, min(32, g1 - g), cols, m, W,
+                                                          lg, lg_max, b, status, s_q[warp],
+                                                          nullptr, nullptr, &nq);
+    if (nq) hits += walk_keys<HIER>(s_q[warp], nq, W, lg, lg_max, b, status);
     credit(w, h0);
   }
 
@@ -279,10 +285,10 @@ __global__ void __launch_bounds__(kOT, 2)
     }
     int TP;
     const int Q = warp_excl_scan(P, &TP);
-    // OWN: the queue arrays (idle in this phase) hold, per pair lane, its
-    // owner lane (s_qh) and, per owner lane, its hits (s_qx)
-    int* pair_owner = s_qh[warp];
-    int* own_hits = s_qx[warp];
+    // OWN: the queue (idle in this phase) holds, per pair lane, its owner
+    // lane and, per owner lane, its hits
+    int* pair_owner = s_q[warp];
+    int* own_hits = s_q[warp] + 32;
     if (OWN) own_hits[lane] = 0;
     for (int base = 0; base < TP; base += 32) {
       const int f = base + lane;
