@@ -295,19 +295,21 @@ def run_ours(a, rank, world, local):
                  "warp_pair_min": hp.warp_pair_min, "measured_ms": hp.measured_ms}
         torch.cuda.synchronize()
 
-    # Steps are pipelined on two streams: a table build runs on s_build
-    # (its one sizing sync waits only for that stream), the probe and the
-    # stream-ordered free on s_probe, so the host queues step k+1 while the
-    # probe of step k runs and never waits for a probe inside the loop.
-    stream = torch.cuda.current_stream()   # s_probe
-    s_build = torch.cuda.Stream()
+    # A step's build and count run back to back on one stream: both fill
+    # every SM, and a build overlapped with the previous count only slowed
+    # both.  e2e steps copy their CSR on a copy stream, so step k+1's H2D
+    # overlaps step k's kernels.  The build's one sizing sync waits for the
+    # previous count; the free is stream-ordered.
+    stream = torch.cuda.current_stream()
+    s_copy = torch.cuda.Stream()
     probe_ms = []
     counts = []
-    in_flight = []   # probe-done events of steps not yet known finished
+    in_flight = []   # done events of steps not yet known finished
 
-    # e2e inputs land in two device buffers used in turn (a buffer is free
-    # again once the step two back has finished, which step() waits for)
+    # e2e inputs land in two device buffers used in turn; a buffer is
+    # rewritten only after the step that last read it has finished
     e2e_bufs = [(torch.empty_like(off), torch.empty_like(cols)) for _ in range(2)]
+    buf_free = [None, None]
     n_e2e = [0]
 
     def step(record=False, off_d=off, cols_d=cols, inputs_from=None, out=None):
@@ -315,17 +317,21 @@ def run_ours(a, rank, world, local):
         # working set in warm-up and in the timed region (no growth there)
         while len(in_flight) >= 2:
             in_flight.pop(0).synchronize()
-        with torch.cuda.stream(s_build):
-            if inputs_from is not None:   # e2e: this step's CSR from pinned host memory
-                off_d, cols_d = e2e_bufs[n_e2e[0] % 2]
-                n_e2e[0] += 1
+        buf = None
+        if inputs_from is not None:   # e2e: this step's CSR from pinned host memory
+            buf = n_e2e[0] % 2
+            n_e2e[0] += 1
+            off_d, cols_d = e2e_bufs[buf]
+            with torch.cuda.stream(s_copy):
+                if buf_free[buf] is not None:
+                    s_copy.wait_event(buf_free[buf])
                 off_d.copy_(inputs_from[0], non_blocking=True)
                 cols_d.copy_(inputs_from[1], non_blocking=True)
-            t = api.Table(off_d, cols_d, alpha=a.alpha, bucket=a.bucket, hierarchical=True,
-                          hash_order=True, stream=s_build)
-            built = torch.cuda.Event()
-            built.record(s_build)
-        stream.wait_event(built)
+                copied = torch.cuda.Event()
+                copied.record(s_copy)
+            stream.wait_event(copied)
+        t = api.Table(off_d, cols_d, alpha=a.alpha, bucket=a.bucket, hierarchical=True,
+                      hash_order=True, stream=stream)
         if record:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -336,12 +342,12 @@ def run_ours(a, rank, world, local):
         if out is not None:
             out.copy_(cnt, non_blocking=True)     # D2H of the step's result
         counts.append(cnt)
-        for x in (t.hash_order, off_d, cols_d):
-            x.record_stream(stream)
         t.free_async(stream)
         done = torch.cuda.Event()
         done.record(stream)
         in_flight.append(done)
+        if buf is not None:
+            buf_free[buf] = done
 
     def barrier():
         if world > 1:
@@ -369,7 +375,6 @@ def run_ours(a, rank, world, local):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        s_build.wait_event(ev0)
         for _ in range(a.steps):
             step(record=True)
         ev1.record(stream)

@@ -37,6 +37,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kTileThreads = 512;  // threads of a tile-build CTA (3 CTAs, 48 warps per SM)
+constexpr int kTileWarps = kTileThreads / 32;
 constexpr int kThreadSetMax = 8;      // sets with deg <= this: thread per set
 constexpr int kTileSmemBudget = 72 * 1024;
 constexpr int kBigFillSmemMax = 64 * 1024;  // buckets whose fill bytes fit smem
@@ -309,7 +311,7 @@ __device__ void extract_set_warp(int l, int b, int32_t* __restrict__ out,
 // ----------------------------------------------------------- tile build --
 
 template <bool HIER>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTileThreads)
     tile_build_kernel(const int32_t* __restrict__ off,
                       const int32_t* __restrict__ elems,
                       const int32_t* __restrict__ len,
@@ -323,6 +325,7 @@ __global__ void __launch_bounds__(kThreads)
   int32_t* S = reinterpret_cast<int32_t*>(smem);
   unsigned char* fill = smem + (size_t)R_max * 4 * b;
   __shared__ int s_run_end;
+  __shared__ int s_span[kTileWarps];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int s0 = tile_first[blockIdx.x], s1 = tile_first[blockIdx.x + 1];
@@ -364,15 +367,15 @@ __global__ void __launch_bounds__(kThreads)
       const int q = R >> 2;
       for (int k = 0; k < b; ++k) {
         int4* P = reinterpret_cast<int4*>(S + (size_t)k * R_max);
-        for (int i = tid; i < q; i += kThreads) P[i] = neg;
+        for (int i = tid; i < q; i += kTileThreads) P[i] = neg;
       }
       int32_t* F = reinterpret_cast<int32_t*>(fill);
-      for (int i = tid; i < q; i += kThreads) F[i] = 0;
+      for (int i = tid; i < q; i += kTileThreads) F[i] = 0;
     }
     __syncthreads();
 
     // 2a. small sets, one thread each.
-    for (int s = u + tid; s < r; s += kThreads) {
+    for (int s = u + tid; s < r; s += kTileThreads) {
       int rs = off[s], d = off[s + 1] - rs;
       if (d > kThreadSetMax || d == 0) continue;
       int lg = 31 - __clz(len[s]);
@@ -380,7 +383,7 @@ __global__ void __launch_bounds__(kThreads)
       insert_set_thread<HIER>(elems + rs, d, lg, lg_max, b, sl, status);
     }
     // 2b. larger sets, one warp each.
-    for (int s = u + warp; s < r; s += kWarps) {
+    for (int s = u + warp; s < r; s += kTileWarps) {
       int rs = off[s], d = off[s + 1] - rs;
       if (d <= kThreadSetMax) continue;
       int lg = 31 - __clz(len[s]);
@@ -397,15 +400,35 @@ __global__ void __launch_bounds__(kThreads)
                    (unsigned)R * 4u);
       bulk_commit();
     }
-    // 4. optional: rows in bucket order, read from the tile.
+    // 4. optional: rows in bucket order, read from the tile.  The run's sets
+    // are consecutive in the tile and their rows consecutive in the CSR, so
+    // the rows in bucket order are the tile's non-empty slots in (bucket,
+    // slot) order, compacted into hash_out[off[u] .. off[r]): each warp
+    // counts a contiguous span of slots, then writes its keys after the
+    // spans before it.
     if (hash_out) {
-      for (int s = u + warp; s < r; s += kWarps) {
-        int rs = off[s], d = off[s + 1] - rs;
-        if (d == 0) continue;
-        int base = (int)(off64[s] - RA);
-        extract_set_warp(len[s], b, hash_out + rs, [&](int bb, int k) {
-          return S[k * R_max + base + bb];
-        });
+      const int total = R * b;
+      const int span = (((total + kTileWarps - 1) / kTileWarps) + 31) & ~31;
+      const int i_lo = min(total, warp * span), i_hi = min(total, i_lo + span);
+      auto slot = [&](int i) {
+        return b == 1 ? S[i] : S[(i % b) * R_max + i / b];
+      };
+      int c = 0;
+      for (int i0 = i_lo; i0 < i_hi; i0 += 32) {
+        const int i = i0 + lane;
+        c += __popc(__ballot_sync(kFull, i < i_hi && slot(i) != -1));
+      }
+      if (lane == 0) s_span[warp] = c;
+      __syncthreads();
+      int w = off[u];
+      for (int k = 0; k < warp; ++k) w += s_span[k];
+      const unsigned lt = lanemask_lt();
+      for (int i0 = i_lo; i0 < i_hi; i0 += 32) {
+        const int i = i0 + lane;
+        const int v = i < i_hi ? slot(i) : -1;
+        const unsigned msk = __ballot_sync(kFull, v != -1);
+        if (v != -1) hash_out[w + __popc(msk & lt)] = v;
+        w += __popc(msk);
       }
     }
     if (tid == 0) bulk_wait_read_all();
@@ -596,7 +619,7 @@ reset_status launch_builds(const reset_table* t, const int32_t* d_off,
     RST_CUDA(cudaFuncSetAttribute(tile_build_kernel<HIER>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)g.smem));
-    note_launch(); tile_build_kernel<HIER><<<n_tiles, kThreads, g.smem, st>>>(
+    note_launch(); tile_build_kernel<HIER><<<n_tiles, kTileThreads, g.smem, st>>>(
         d_off, d_elems, t->d_len, t->d_off64, d_tile_first, t->bucket_num,
         t->bucket, t->lg_max, g.R_max, g.LT, t->d_table, d_hash_out,
         t->d_status);
