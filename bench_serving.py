@@ -299,7 +299,6 @@ def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None, window=40
     returns (results, wall seconds, list of requests used)."""
     from collections import deque
     from reset_b200.server import now_ns
-    tickets = []
     used = []
     t0 = time.perf_counter()
     if rate is None:
@@ -313,20 +312,48 @@ def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None, window=40
         while pend:
             res.append(srv.wait(pend.popleft()))
         return res, time.perf_counter() - t0, used
-    else:
-        base = now_ns() + 2_000_000
-        t = 0.0
-        i = 0
-        while t < seconds:
-            t += rng.exponential(1.0 / rate)
-            q = reqs[i % len(reqs)]
-            i += 1
-            at = base + int(t * 1e9)
-            while now_ns() < at:
-                pass
-            tickets.append(submit(q, at))
-            used.append(q)
-    res = [srv.wait(tk) for tk in tickets]
+    # Poisson arrivals: a consumer thread waits for the results in order and
+    # releases each at once (as a client would), so completed results do not
+    # pile up in the server's pinned result arena while requests arrive.
+    # Result arrays are copied out for the first `checked` results only, and
+    # the interpreter hands over between the threads every 0.2 ms, so the
+    # consumer does not delay the submitting thread's arrivals.
+    import queue
+    import sys
+    import threading
+    ready = queue.Queue()
+    res = []
+    checked = 200
+
+    def consume():
+        while True:
+            tk = ready.get()
+            if tk is None:
+                return
+            res.append(srv.wait(tk, copy_out=len(res) < checked))
+
+    switch = sys.getswitchinterval()
+    sys.setswitchinterval(0.0002)
+    th = threading.Thread(target=consume, daemon=True)
+    th.start()
+    base = now_ns() + 2_000_000
+    t = 0.0
+    i = 0
+    while t < seconds:
+        t += rng.exponential(1.0 / rate)
+        q = reqs[i % len(reqs)]
+        i += 1
+        at = base + int(t * 1e9)
+        gap = at - now_ns()
+        if gap > 400_000:   # sleep (releasing the interpreter) until ~0.2 ms before
+            time.sleep((gap - 200_000) / 1e9)
+        while now_ns() < at:
+            pass
+        ready.put(submit(q, at))
+        used.append(q)
+    ready.put(None)
+    th.join()
+    sys.setswitchinterval(switch)
     return res, time.perf_counter() - t0, used
 
 

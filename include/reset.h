@@ -412,7 +412,11 @@ typedef struct {
                                  in a batch of its own, and such batches hold
                                  at most streams - 1 slots, so lighter requests
                                  never wait behind one (they may pass it)   */
-  int32_t reserved[6];
+  int64_t pinned_result_bytes; /* pinned host arena that IR results land in
+                                 and are handed out from without a copy
+                                 until released (default 256 MiB); results
+                                 that do not fit are copied out           */
+  int32_t reserved[4];
 } reset_server_config;
 
 enum {

@@ -47,7 +47,7 @@ class TableView(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("streams", C.c_int32), ("max_batch_requests", C.c_int32),
                 ("mem_budget_bytes", C.c_int64), ("max_batch_cost", C.c_int64),
-                ("reserved", C.c_int32 * 6)]
+                ("pinned_result_bytes", C.c_int64), ("reserved", C.c_int32 * 4)]
 
 
 class Request(C.Structure):

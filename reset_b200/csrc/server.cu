@@ -24,6 +24,8 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <iterator>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -178,17 +180,71 @@ struct Index {
   int32_t n() const { return (int32_t)h_off.size() - 1; }
 };
 
-// A pinned host block holding the IR survivors of one batch; requests keep
-// it alive (shared ownership) until they are released, so results are
-// handed out without copying.  Blocks are reused from the server's pool.
-struct PinnedBlock {
-  void* p = nullptr;
-  size_t cap = 0;
-  ~PinnedBlock() {
-    if (p) cudaFreeHost(p);
+// The pinned host arena IR survivors are copied into: one allocation made
+// when the server starts, carved first-fit into 256-byte aligned ranges.
+// A batch's range is a lease its requests share; the last release returns
+// it, so results are handed out without copying and no pinned memory is
+// allocated or freed (cudaFreeHost synchronises the device) while serving.
+class PinnedArena {
+ public:
+  ~PinnedArena() {
+    if (base_) cudaFreeHost(base_);
   }
+  cudaError_t init(size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    cudaError_t e = cudaHostAlloc(&base_, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      base_ = nullptr;
+      return e;
+    }
+    free_[0] = bytes;
+    return cudaSuccess;
+  }
+  // A range of `bytes`, or nullptr when none is free.
+  char* take(size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_[off + bytes] = len - bytes;
+      return static_cast<char*>(base_) + off;
+    }
+    return nullptr;
+  }
+  void give(char* p, size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    size_t off = (size_t)(p - static_cast<char*>(base_));
+    std::lock_guard<std::mutex> lk(mu_);
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + bytes == next->first) {  // merge right
+      bytes += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {  // merge left
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += bytes;
+        return;
+      }
+    }
+    free_[off] = bytes;
+  }
+
+ private:
+  void* base_ = nullptr;
+  std::mutex mu_;
+  std::map<size_t, size_t> free_;  // offset -> length
 };
-using BlockP = std::shared_ptr<PinnedBlock>;
+
+struct Lease {
+  PinnedArena* arena;
+  char* p;
+  size_t bytes;
+  ~Lease() { arena->give(p, bytes); }
+};
+using LeaseP = std::shared_ptr<Lease>;
 
 struct Req {
   uint64_t id = 0;
@@ -199,8 +255,10 @@ struct Req {
   int64_t cost = 0;  // estimated probes (batch formation)
   int64_t aux = 0;  // IR: df(first term); TC: number of (v, w) pairs; RAW: len
   reset_status status = RESET_OK;
-  BlockP docs_block;               // IR: survivors live in this pinned block, or
-  std::vector<int32_t> docs_copy;  // in this copy when no block was free
+  // IR: what holds the survivors `docs` points into -- an arena lease, or
+  // the batch's pageable buffer when the arena was full -- shared by the
+  // batch's requests
+  std::shared_ptr<const void> docs_owner;
   const int32_t* docs = nullptr;
   std::vector<int64_t> values;
   std::vector<uint8_t> flags;
@@ -215,20 +273,27 @@ struct Req {
 };
 using ReqP = std::shared_ptr<Req>;
 
+// A growable pinned staging buffer of one slot.  Outgrown buffers are kept
+// until the server is destroyed: cudaFreeHost synchronises the device, which
+// would stall every batch in flight.
 struct Pinned {
   void* p = nullptr;
   size_t cap = 0;
+  std::vector<void*> retired;
   cudaError_t ensure(size_t n) {
     if (n <= cap) return cudaSuccess;
     const size_t c = std::max(n, cap * 2);
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-    cudaError_t e = cudaHostAlloc(&p, c, cudaHostAllocDefault);
-    if (e == cudaSuccess) cap = c;
-    return e;
+    void* q = nullptr;
+    cudaError_t e = cudaHostAlloc(&q, c, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    if (p) retired.push_back(p);
+    p = q;
+    cap = c;
+    return cudaSuccess;
   }
   void release() {
+    for (void* q : retired) cudaFreeHost(q);
+    retired.clear();
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
@@ -261,8 +326,10 @@ struct Batch {
   int phase = 0;  // 0: kernels + small outputs in flight; 1: IR survivors in flight
   bool heavy = false;  // one request above the cost cap
   cudaStream_t st = nullptr;  // the slot stream the batch runs on
-  BlockP res;     // pinned block receiving the IR survivors (phase 1), or
-  const int32_t* res_ptr = nullptr;  // the slot's own buffer (then copied out)
+  // where the IR survivors land (phase 1): an arena range, or a pageable
+  // buffer of the batch when the arena is full
+  std::shared_ptr<const void> res;
+  const int32_t* res_ptr = nullptr;
   reset_status status = RESET_OK;
 };
 
@@ -270,10 +337,11 @@ struct Slot {
   cudaStream_t st = nullptr;     // light batches (highest priority)
   cudaStream_t st_lo = nullptr;  // heavy batches (lowest priority)
   cudaEvent_t ev = nullptr;
-  Pinned in, out, res;
+  Pinned in, out;
   void* arena = nullptr;  // device buffer reused by this slot's batches
   size_t arena_cap = 0;
-  std::unique_ptr<Batch> batch;  // set while in flight
+  std::unique_ptr<Batch> batch;  // set while its kernels or copies are in flight
+  bool busy = false;  // a batch is in flight or with a finisher thread
 };
 
 }  // namespace
@@ -285,18 +353,23 @@ struct reset_server {
   std::vector<Index> indexes;
   std::vector<Slot> slots;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_fin;
   std::deque<ReqP> pending;
   std::unordered_map<uint64_t, ReqP> reqs;
   uint64_t next_id = 1;
   int64_t next_batch = 0;
   int64_t budget = 0, in_use = 0;
-  bool stop = false;
+  bool stop = false, fin_stop = false;
   std::thread worker;
+  // Finished kernels (slot, batch) for the finisher threads, which enqueue
+  // the IR survivor copies and hand results out, so that host copies of
+  // large results never hold up the scheduler thread.
+  std::deque<std::pair<int, std::unique_ptr<Batch>>> finished;
+  std::vector<std::thread> finishers;
   int64_t n_done = 0, n_batches = 0, sum_batch = 0, max_batch = 0;
   int64_t max_in_use = 0, max_inflight = 0, inflight = 0, heavy_inflight = 0;
   int64_t launch_ns = 0, batch_ns = 0;
-  std::vector<BlockP> blocks;  // pinned result blocks (free when only the pool holds one)
+  PinnedArena results;  // IR survivors handed out without a copy
 };
 
 namespace {
@@ -704,12 +777,9 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
         const int32_t* src = bt.res_ptr + g.dense_host + o;
         if (c == 0) {
           r->docs = nullptr;
-        } else if (bt.res) {  // hand out the pinned block itself
-          r->docs_block = bt.res;
+        } else {  // hand out the batch's buffer itself
+          r->docs_owner = bt.res;
           r->docs = src;
-        } else {              // the slot's buffer is reused: copy
-          r->docs_copy.assign(src, src + c);
-          r->docs = r->docs_copy.data();
         }
         break;
       }
@@ -762,27 +832,23 @@ void unpack_batch(const reset_server* s, Slot& sl, Batch& bt) {
   }
 }
 
-// After the kernels: copies every IR group's packed survivors (sizes now
-// known on the host) into the slot's pinned result buffer.  Returns true if
-// copies were enqueued (the batch completes at the next event).
-// A free pinned block of at least `bytes` from the pool (under the server
-// lock), a new one while the pool holds fewer than two per stream, else
-// nullptr (the batch then lands in the slot's buffer and is copied out).
-BlockP take_block(reset_server* s, size_t bytes) {
-  std::lock_guard<std::mutex> lk(s->mu);
-  BlockP best;
-  for (auto& b : s->blocks)
-    if (b.use_count() == 1 && b->cap >= bytes && (!best || b->cap < best->cap)) best = b;
-  if (best) return best;
-  if (s->blocks.size() >= 2 * s->slots.size()) return nullptr;
-  auto b = std::make_shared<PinnedBlock>();
-  const size_t cap = std::max(bytes, (size_t)(1u << 20));
-  if (cudaHostAlloc(&b->p, cap, cudaHostAllocDefault) != cudaSuccess) return nullptr;
-  b->cap = cap;
-  s->blocks.push_back(b);
-  return b;
+// A lease of `bytes` in the server's result arena, or nullptr when the
+// arena is full (results still held by clients).
+LeaseP take_lease(reset_server* s, size_t bytes) {
+  char* p = s->results.take(bytes);
+  if (!p) return nullptr;
+  try {
+    return LeaseP(new Lease{&s->results, p, bytes});
+  } catch (const std::bad_alloc&) {
+    s->results.give(p, bytes);
+    return nullptr;
+  }
 }
 
+// After the kernels (finisher thread): copies every IR group's packed
+// survivors (sizes now known on the host) into an arena range, or, when the
+// arena is full, into a pageable buffer of the batch.  Returns true if
+// copies were enqueued (the batch completes at the next event).
 bool enqueue_results(reset_server* s, Slot& sl, Batch& bt) {
   const char* hp = static_cast<const char*>(sl.out.p);
   size_t total = 0;
@@ -793,15 +859,22 @@ bool enqueue_results(reset_server* s, Slot& sl, Batch& bt) {
     total += (size_t)g.dense_n;
   }
   if (total == 0) return false;
-  bt.res = take_block(s, 4 * total);
-  if (bt.res) {
-    bt.res_ptr = static_cast<const int32_t*>(bt.res->p);
+  if (LeaseP lease = take_lease(s, 4 * total)) {
+    bt.res_ptr = reinterpret_cast<const int32_t*>(lease->p);
+    bt.res = std::move(lease);
   } else {
-    if (sl.res.ensure(4 * total) != cudaSuccess) {
-      bt.status = cuda_fail(cudaErrorMemoryAllocation, "pinned result buffer", __FILE__, __LINE__);
+    // Arena full (clients still hold results): a pageable buffer of the
+    // batch.  Its copies return once done (pageable destination), which
+    // only this finisher thread waits for; pinned memory is never
+    // allocated while serving (cudaHostAlloc can stall other CUDA calls).
+    try {
+      auto buf = std::make_shared<std::vector<int32_t>>(total);
+      bt.res_ptr = buf->data();
+      bt.res = std::move(buf);
+    } catch (const std::bad_alloc&) {
+      bt.status = RESET_ERR_OOM;
       return false;
     }
-    bt.res_ptr = static_cast<const int32_t*>(sl.res.p);
   }
   const char* dp = static_cast<const char*>(bt.d_buf);
   for (auto& g : bt.groups) {
@@ -828,39 +901,21 @@ void worker_main(reset_server* s) {
   std::unique_lock<std::mutex> lk(s->mu);
   for (;;) {
     bool progressed = false;
-    // completions
-    for (auto& sl : s->slots) {
+    // completions go to the finisher threads (the slot stays busy)
+    for (size_t i = 0; i < s->slots.size(); ++i) {
+      Slot& sl = s->slots[i];
       if (!sl.batch) continue;
       cudaError_t q = cudaEventQuery(sl.ev);
       if (q == cudaErrorNotReady) continue;
       std::unique_ptr<Batch> bt = std::move(sl.batch);
-      lk.unlock();
       if (q != cudaSuccess) bt->status = cuda_fail(q, "server batch", __FILE__, __LINE__);
-      if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(s, sl, *bt)) {
-        lk.lock();
-        sl.batch = std::move(bt);  // survivors in flight
-        progressed = true;
-        continue;
-      }
-      if (bt->status == RESET_OK) unpack_batch(s, sl, *bt);
-      const int64_t t = now_ns();
-      lk.lock();
-      s->batch_ns += t - bt->t_launch;
-      for (auto& r : bt->reqs) {
-        if (bt->status != RESET_OK) r->status = bt->status;
-        r->t_done = t;
-        r->done = true;
-        ++s->n_done;
-      }
-      s->in_use -= bt->reserved;
-      --s->inflight;
-      if (bt->heavy) --s->heavy_inflight;
+      s->finished.emplace_back((int)i, std::move(bt));
+      s->cv_fin.notify_one();
       progressed = true;
-      s->cv_done.notify_all();
     }
     // launches
     for (auto& sl : s->slots) {
-      if (sl.batch || s->pending.empty()) continue;
+      if (sl.busy || s->pending.empty()) continue;
       auto bt = std::make_unique<Batch>();
       int64_t bytes = 0, cost = 0;
       // Requests are taken in arrival order while the batch's estimated
@@ -922,6 +977,7 @@ void worker_main(reset_server* s) {
         r->batch_id = bt->id;
         r->batch_size = (int32_t)bt->reqs.size();
       }
+      sl.busy = true;
       lk.unlock();
       bt->t_launch = t;
       reset_status rs = launch_batch(s, sl, *bt);
@@ -945,6 +1001,45 @@ void worker_main(reset_server* s) {
   }
 }
 
+// Finisher thread: takes batches whose event completed; a phase-0 batch with
+// IR survivors gets their copies enqueued and goes back in flight, any other
+// has its results handed to its requests, and its slot is freed.
+void finisher_main(reset_server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_fin.wait(lk, [s] { return s->fin_stop || !s->finished.empty(); });
+    if (s->finished.empty()) break;  // fin_stop: the scheduler has drained
+    const int i = s->finished.front().first;
+    std::unique_ptr<Batch> bt = std::move(s->finished.front().second);
+    s->finished.pop_front();
+    Slot& sl = s->slots[i];
+    lk.unlock();
+    if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(s, sl, *bt)) {
+      lk.lock();
+      sl.batch = std::move(bt);  // survivors in flight; the scheduler polls the event
+      s->cv_work.notify_one();
+      continue;
+    }
+    if (bt->status == RESET_OK) unpack_batch(s, sl, *bt);
+    const int64_t t = now_ns();
+    lk.lock();
+    s->batch_ns += t - bt->t_launch;
+    for (auto& r : bt->reqs) {
+      if (bt->status != RESET_OK) r->status = bt->status;
+      r->t_done = t;
+      r->done = true;
+      ++s->n_done;
+    }
+    s->in_use -= bt->reserved;
+    --s->inflight;
+    if (bt->heavy) --s->heavy_inflight;
+    sl.busy = false;
+    s->cv_done.notify_all();
+    s->cv_work.notify_one();
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -956,6 +1051,7 @@ void reset_server_config_default(reset_server_config* c) {
   c->max_batch_requests = 1024;
   c->max_batch_cost = int64_t(1) << 22;
   c->mem_budget_bytes = 0;
+  c->pinned_result_bytes = int64_t(256) << 20;
 }
 
 int64_t reset_now_ns(void) { return now_ns(); }
@@ -970,6 +1066,8 @@ reset_status reset_server_create(const reset_server_config* cfg, reset_server** 
   if (c.max_batch_requests < 1) return arg_fail("max_batch_requests must be >= 1");
   if (c.mem_budget_bytes < 0) return arg_fail("negative memory budget");
   if (c.max_batch_cost < 0) return arg_fail("negative max_batch_cost");
+  if (c.pinned_result_bytes < 0) return arg_fail("negative pinned_result_bytes");
+  if (c.pinned_result_bytes == 0) c.pinned_result_bytes = int64_t(256) << 20;
   std::unique_ptr<reset_server> s;
   try {
     s.reset(new reset_server());
@@ -998,10 +1096,20 @@ reset_status reset_server_create(const reset_server_config* cfg, reset_server** 
     RST_CUDA(cudaStreamCreateWithPriority(&sl.st_lo, cudaStreamNonBlocking, prio_lo));
     RST_CUDA(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
   }
+  RST_CUDA(s->results.init((size_t)c.pinned_result_bytes));
+  // finisher threads (one per slot, at most four), then the scheduler
   try {
+    const int nf = std::min(c.streams, 4);
+    for (int i = 0; i < nf; ++i) s->finishers.emplace_back(finisher_main, s.get());
     s->worker = std::thread(worker_main, s.get());
   } catch (...) {
-    return arg_fail("cannot start the server thread");
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stop = s->fin_stop = true;
+    }
+    s->cv_fin.notify_all();
+    for (auto& f : s->finishers) f.join();
+    return arg_fail("cannot start the server threads");
   }
   *out = s.release();
   return RESET_OK;
@@ -1136,7 +1244,14 @@ reset_status reset_server_destroy(reset_server* s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
-  if (s->worker.joinable()) s->worker.join();
+  if (s->worker.joinable()) s->worker.join();  // returns once nothing is in flight
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->fin_stop = true;
+  }
+  s->cv_fin.notify_all();
+  for (auto& f : s->finishers)
+    if (f.joinable()) f.join();
   cudaError_t e = cudaSuccess;
   for (auto& sl : s->slots) {
     for (cudaStream_t* p : {&sl.st, &sl.st_lo}) {
@@ -1149,10 +1264,8 @@ reset_status reset_server_destroy(reset_server* s) {
     if (sl.arena) cudaFree(sl.arena);
     sl.in.release();
     sl.out.release();
-    sl.res.release();
   }
-  s->reqs.clear();
-  s->blocks.clear();
+  s->reqs.clear();  // their leases go back to the arena, freed with the server
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   if (e != cudaSuccess) return cuda_fail(e, "reset_server_destroy", __FILE__, __LINE__);

@@ -253,8 +253,11 @@ __device__ __forceinline__ int owner_lane_n(int P, int f) {
 // the hash) and outlives the call: *nq_keep carries its length from call to
 // call over one staged table, and the caller walks the rest with walk_keys
 // before the table changes.
+//
+// PF: the next R chunks of keys are loaded before the current ones are
+// probed (software pipelining across rounds).
 template <bool HIER, int R, bool PAIRS = false, int NR = 32, int QCAP = kQueue,
-          bool KEEP = false>
+          bool KEEP = false, bool PF = false>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
@@ -302,9 +305,9 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
     __syncwarp();
     nq = 0;
   };
-  for (int base = 0; base < total; base += 32 * R) {
-    int x[R][4];
-    int kk[R];  // the row (lane index) of this lane's chunk, -1 if none
+  // Loads the R chunks of rounds [base, base + 32R) of this lane: keys in
+  // x (-2 outside rows), rows in kk (-1 if none).
+  auto load = [&](int base, int (&x)[R][4], int (&kk)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       kk[r] = -1;
@@ -341,6 +344,9 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         }
       }
     }
+  };
+  // Probes the keys of rounds [base, base + 32R).
+  auto probe = [&](int base, const int (&x)[R][4], const int (&kk)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (base + r * 32 >= total) break;  // warp-uniform
@@ -370,6 +376,29 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         const unsigned sum = __reduce_add_sync(grp, hr);
         if (kk[r] >= 0 && lane == __ffs(grp) - 1 && sum) atomicAdd(s_cnt + kk[r], (int)sum);
       }
+    }
+  };
+  if (PF) {
+    // the next R chunks are loaded before this round's keys are probed,
+    // so their latency hides behind the probes
+    int xn[R][4], kn[R];
+    if (total > 0) load(0, xn, kn);
+    for (int base = 0; base < total; base += 32 * R) {
+      int x[R][4], kk[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        kk[r] = kn[r];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[r][j] = xn[r][j];
+      }
+      if (base + 32 * R < total) load(base + 32 * R, xn, kn);
+      probe(base, x, kk);
+    }
+  } else {
+    for (int base = 0; base < total; base += 32 * R) {
+      int x[R][4], kk[R];
+      load(base, x, kk);
+      probe(base, x, kk);
     }
   }
   if (KEEP)

@@ -142,6 +142,11 @@ __global__ void __launch_bounds__(kOT)
 
 // OWN: every owner's hits are also added to owner_hits[owner] (per-graph
 // counts of a batch of disjoint graphs are sums over their vertex ranges).
+// Rounds of 32 key chunks a warp keeps in flight, and whether the next
+// rounds' keys are loaded before the current ones are probed.
+constexpr int kOwnerRounds = 4;
+constexpr bool kOwnerPrefetch = false;
+
 template <bool HIER, int R, bool OWN = false>
 __global__ void __launch_bounds__(kOT, 2)
     tc_owner_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(kOT, 2)
   // batches a warp takes from one staged table and walked once three rounds'
   // worth is queued (or the table changes), so walks run with full warps
   constexpr int QCAP = 4 * kQueue;
+  constexpr bool PF = kOwnerPrefetch;
   __shared__ int s_q[kOW][QCAP];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= kOW) mbar_init(&s_bar[tid]);
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(kOT, 2)
       if (lane == 0) g = g0 + atomicAdd(&s_next, kGrab);
       g = __shfl_sync(kFull, g, 0);
       if (g >= g1) break;
-      hits += staged_keys<HIER, R, false, kGrab, QCAP, true>(
+      hits += staged_keys<HIER, R, false, kGrab, QCAP, true, PF>(
           ent + g, min(kGrab, g1 - g), cols, m, sm, lg, lg_max, b, status, s_q[warp], nullptr,
           nullptr, &nq);
     }
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(kOT, 2)
     const unsigned long long h0 = hits;
     int nq = 0;
     for (int g = g0; g < g1; g += 32)
-      hits += staged_keys<HIER, R, false, 32, QCAP, true>(ent + g, min(32, g1 - g), cols, m, W,
+      hits += staged_keys<HIER, R, false, 32, QCAP, true, PF>(ent + g, min(32, g1 - g), cols, m, W,
                                                           lg, lg_max, b, status, s_q[warp],
                                                           nullptr, nullptr, &nq);
     if (nq) hits += walk_keys<HIER>(s_q[warp], nq, W, lg, lg_max, b, status);
@@ -390,7 +396,7 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   if (e == cudaSuccess) {
     const size_t smem = sizeof(int) * kCtaTab;
     const bool own = owner_hits != nullptr;
-#define OWN_K(H, O) tc_owner_kernel<H, 4, O>
+#define OWN_K(H, O) tc_owner_kernel<H, kOwnerRounds, O>
     const void* k = t->hier ? (own ? (const void*)OWN_K(true, true) : (const void*)OWN_K(true, false))
                             : (own ? (const void*)OWN_K(false, true)
                                    : (const void*)OWN_K(false, false));

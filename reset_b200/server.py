@@ -46,7 +46,8 @@ def _i32(a) -> np.ndarray:
 
 class Server:
     def __init__(self, streams: int = 4, max_batch_requests: int = 1024,
-                 mem_budget_bytes: int = 0, max_batch_cost: Optional[int] = None):
+                 mem_budget_bytes: int = 0, max_batch_cost: Optional[int] = None,
+                 pinned_result_bytes: Optional[int] = None):
         L = load()
         cfg = ServerConfig()
         L.reset_server_config_default(C.byref(cfg))
@@ -55,6 +56,8 @@ class Server:
         cfg.mem_budget_bytes = mem_budget_bytes
         if max_batch_cost is not None:   # estimated probes per batch; 0 = no limit
             cfg.max_batch_cost = max_batch_cost
+        if pinned_result_bytes is not None:   # host arena for IR results
+            cfg.pinned_result_bytes = pinned_result_bytes
         h = C.c_void_p()
         check(L.reset_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -109,13 +112,20 @@ class Server:
     def submit_raw(self, a, b, arrival_ns: int = 0) -> int:
         return self.submit(RAW, 0, a, b, arrival_ns=arrival_ns)
 
-    def wait(self, ticket: int, timeout_ms: int = -1, release: bool = True) -> ServedResult:
+    def wait(self, ticket: int, timeout_ms: int = -1, release: bool = True,
+             copy_out: bool = True) -> ServedResult:
+        """Blocks until the request is done.  copy_out=False skips copying
+        the result arrays (docs, values and flags are then None; the count
+        and timings are kept)."""
         r = Result()
         check(load().reset_server_wait(self._h, ticket, timeout_ms, C.byref(r)))
-        docs = np.ctypeslib.as_array(r.docs, shape=(r.ndocs,)).copy() if r.ndocs else None
-        vals = np.ctypeslib.as_array(r.values, shape=(r.nvalues,)).copy() if r.nvalues else None
-        flags = (np.ctypeslib.as_array(r.flags, shape=(r.nvalues,)).copy()
-                 if r.nvalues and r.flags else None)
+        docs = vals = flags = None
+        if copy_out:
+            docs = np.ctypeslib.as_array(r.docs, shape=(r.ndocs,)).copy() if r.ndocs else None
+            vals = (np.ctypeslib.as_array(r.values, shape=(r.nvalues,)).copy()
+                    if r.nvalues else None)
+            flags = (np.ctypeslib.as_array(r.flags, shape=(r.nvalues,)).copy()
+                     if r.nvalues and r.flags else None)
         out = ServedResult(r.status, r.kind, r.count, docs, vals, flags, r.queue_us,
                            r.service_us, r.latency_us, r.batch_id, r.batch_size)
         if release:

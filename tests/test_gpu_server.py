@@ -153,6 +153,40 @@ def test_mix_matches_oracle_and_alone(S, world):
                 assert (a is None and b is None) or np.array_equal(a, b)
 
 
+def test_results_when_the_pinned_arena_is_full(S, world):
+    """IR results land in the pinned result arena and are handed out without
+    a copy; while clients hold the arena full, later results land in
+    pageable buffers instead.  Both give the oracle's lists, including when
+    a second thread waits and releases while requests are submitted."""
+    import queue
+    import threading
+    reqs = [q for q in world["reqs"] if q[0] == "ir"]
+    assert sum(q[2].size for q in reqs) * 4 > 8192      # the arena cannot hold all
+    with S.Server(streams=4, max_batch_requests=8, pinned_result_bytes=8192) as srv:
+        ix = _register(srv, world)
+        held = [srv.wait(_submit(srv, ix, q), release=False) for q in reqs[:4]]
+        tickets = [_submit(srv, ix, q) for q in reqs]
+        for q, t in zip(reqs, tickets):
+            _check(q, srv.wait(t))
+        for q, r in zip(reqs[:4], held):
+            _check(q, r)
+    with S.Server(streams=4, max_batch_requests=8, pinned_result_bytes=1 << 16) as srv:
+        ix = _register(srv, world)
+        ready, got = queue.Queue(), []
+
+        def consume():
+            while (tk := ready.get()) is not None:
+                got.append(srv.wait(tk))
+        th = threading.Thread(target=consume)
+        th.start()
+        for q in reqs * 3:
+            ready.put(_submit(srv, ix, q))
+        ready.put(None)
+        th.join()
+    for q, r in zip(reqs * 3, got):
+        _check(q, r)
+
+
 def test_memory_budget_admission(S, world):
     reqs = [q for q in world["reqs"] if q[0] != "raw"]
     budget = 256 * 1024
