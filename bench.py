@@ -414,13 +414,17 @@ def run_ours(a, rank, world, local):
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg_bytes / (probe_avg / 1e3) / 1e9
-    traffic = None
+    # DRAM bytes per launch of the count kernel from a committed ncu record
+    # of the same method, scale and slots per bucket (alpha within 0.05)
+    traffic, traffic_note = None, None
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_kernel_rmat_traffic.json")))
-        for rec in prof["records"]:
-            if (rec["scale"] == a.scale and abs(rec["alpha"] - a.alpha) < 1e-6
-                    and rec["bucket"] == a.bucket):
-                traffic = rec["dram_bytes_per_launch"]
+        prof = json.load(open(os.path.join(ROOT, "profiles", "tc_owner_kernel_traffic.json")))
+        if a.tc_method in (0, 3):
+            for rec in prof["records"]:
+                if (rec["scale"] == a.scale and abs(rec["alpha"] - a.alpha) <= 0.05 + 1e-9
+                        and rec["bucket"] == a.bucket):
+                    traffic = rec["dram_bytes_per_launch"]
+                    traffic_note = rec["how"]
     except Exception:
         pass
 
@@ -453,6 +457,7 @@ def run_ours(a, rank, world, local):
                      "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": traffic,
+                     "traffic_source": traffic_note,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": launches,
     }

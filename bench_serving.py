@@ -332,8 +332,11 @@ def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None, window=40
                 return
             res.append(srv.wait(tk, copy_out=len(res) < checked))
 
+    import gc
     switch = sys.getswitchinterval()
     sys.setswitchinterval(0.0002)
+    gc_was = gc.isenabled()
+    gc.disable()   # a full collection over the results pauses the arrivals
     th = threading.Thread(target=consume, daemon=True)
     th.start()
     base = now_ns() + 2_000_000
@@ -354,6 +357,8 @@ def _serve_phase(srv, reqs, submit, rate=None, seconds=None, rng=None, window=40
     ready.put(None)
     th.join()
     sys.setswitchinterval(switch)
+    if gc_was:
+        gc.enable()
     return res, time.perf_counter() - t0, used
 
 

@@ -469,7 +469,9 @@ typedef struct {
   double launch_host_us;  /* host time spent packing and launching batches  */
   double batch_us;        /* sum over batches of launch -> results unpacked */
   int64_t arena_bytes;    /* device buffers the slots keep for reuse        */
-  int64_t reserved[1];
+  double max_launch_us;   /* longest host time packing + launching a batch  */
+  double max_finish_us;   /* longest host time handing a batch's results out */
+  int64_t reserved[2];
 } reset_server_counters;
 
 void reset_server_config_default(reset_server_config *cfg);

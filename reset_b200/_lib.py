@@ -75,7 +75,8 @@ class ServerCounters(C.Structure):
                 ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64),
                 ("max_in_use_bytes", C.c_int64), ("mean_batch", C.c_double),
                 ("launch_host_us", C.c_double), ("batch_us", C.c_double),
-                ("arena_bytes", C.c_int64), ("reserved", C.c_int64 * 1)]
+                ("arena_bytes", C.c_int64), ("max_launch_us", C.c_double),
+                ("max_finish_us", C.c_double), ("reserved", C.c_int64 * 2)]
 
 
 P = C.c_void_p

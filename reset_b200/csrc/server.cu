@@ -368,7 +368,7 @@ struct reset_server {
   std::vector<std::thread> finishers;
   int64_t n_done = 0, n_batches = 0, sum_batch = 0, max_batch = 0;
   int64_t max_in_use = 0, max_inflight = 0, inflight = 0, heavy_inflight = 0;
-  int64_t launch_ns = 0, batch_ns = 0;
+  int64_t launch_ns = 0, batch_ns = 0, max_launch_ns = 0, max_finish_ns = 0;
   PinnedArena results;  // IR survivors handed out without a copy
 };
 
@@ -988,6 +988,7 @@ void worker_main(reset_server* s) {
       }
       lk.lock();
       s->launch_ns += t_launched - t;
+      s->max_launch_ns = std::max(s->max_launch_ns, t_launched - t);
       sl.batch = std::move(bt);
       progressed = true;
     }
@@ -1015,8 +1016,11 @@ void finisher_main(reset_server* s) {
     s->finished.pop_front();
     Slot& sl = s->slots[i];
     lk.unlock();
+    const int64_t t0 = now_ns();
     if (bt->status == RESET_OK && bt->phase == 0 && enqueue_results(s, sl, *bt)) {
+      const int64_t t1 = now_ns();
       lk.lock();
+      s->max_finish_ns = std::max(s->max_finish_ns, t1 - t0);
       sl.batch = std::move(bt);  // survivors in flight; the scheduler polls the event
       s->cv_work.notify_one();
       continue;
@@ -1024,6 +1028,7 @@ void finisher_main(reset_server* s) {
     if (bt->status == RESET_OK) unpack_batch(s, sl, *bt);
     const int64_t t = now_ns();
     lk.lock();
+    s->max_finish_ns = std::max(s->max_finish_ns, t - t0);
     s->batch_ns += t - bt->t_launch;
     for (auto& r : bt->reqs) {
       if (bt->status != RESET_OK) r->status = bt->status;
@@ -1231,6 +1236,8 @@ reset_status reset_server_stats(reset_server* s, reset_server_counters* st) {
   st->max_in_use_bytes = s->max_in_use;
   st->launch_host_us = s->launch_ns / 1e3;
   st->batch_us = s->batch_ns / 1e3;
+  st->max_launch_us = s->max_launch_ns / 1e3;
+  st->max_finish_us = s->max_finish_ns / 1e3;
   int64_t arena = 0;
   for (auto& sl : s->slots) arena += (int64_t)sl.arena_cap;
   st->arena_bytes = arena;

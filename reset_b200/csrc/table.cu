@@ -39,6 +39,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kTileThreads = 512;  // threads of a tile-build CTA (3 CTAs, 48 warps per SM)
 constexpr int kTileWarps = kTileThreads / 32;
+constexpr bool kTileDynamic = true;  // warps take a tile's larger sets from a cursor
 constexpr int kThreadSetMax = 8;      // sets with deg <= this: thread per set
 constexpr int kTileSmemBudget = 72 * 1024;
 constexpr int kBigFillSmemMax = 64 * 1024;  // buckets whose fill bytes fit smem
@@ -326,6 +327,7 @@ __global__ void __launch_bounds__(kTileThreads)
   unsigned char* fill = smem + (size_t)R_max * 4 * b;
   __shared__ int s_run_end;
   __shared__ int s_span[kTileWarps];
+  __shared__ int s_wnext;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int s0 = tile_first[blockIdx.x], s1 = tile_first[blockIdx.x + 1];
@@ -371,6 +373,7 @@ __global__ void __launch_bounds__(kTileThreads)
       }
       int32_t* F = reinterpret_cast<int32_t*>(fill);
       for (int i = tid; i < q; i += kTileThreads) F[i] = 0;
+      if (tid == 0) s_wnext = 0;
     }
     __syncthreads();
 
@@ -382,8 +385,17 @@ __global__ void __launch_bounds__(kTileThreads)
       SmemSlots sl{S, R_max, fill, (int)(off64[s] - RA)};
       insert_set_thread<HIER>(elems + rs, d, lg, lg_max, b, sl, status);
     }
-    // 2b. larger sets, one warp each.
-    for (int s = u + warp; s < r; s += kTileWarps) {
+    // 2b. larger sets, one warp each, taken from a shared cursor (a fixed
+    // round-robin left warps with one long set waiting at the barrier)
+    for (int wround = 0;; ++wround) {
+      int s = 0;
+      if (kTileDynamic) {
+        if (lane == 0) s = u + atomicAdd(&s_wnext, 1);
+        s = __shfl_sync(kFull, s, 0);
+      } else {
+        s = u + warp + kTileWarps * wround;
+      }
+      if (s >= r) break;
       int rs = off[s], d = off[s + 1] - rs;
       if (d <= kThreadSetMax) continue;
       int lg = 31 - __clz(len[s]);
