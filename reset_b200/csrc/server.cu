@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <iterator>
@@ -599,8 +601,10 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   bt.d_bytes = p;
 
   // ---- pinned input
+  const int64_t t_plan = now_ns();
   if (sl.in.ensure(bt.in_bytes) != cudaSuccess || sl.out.ensure(bt.out_end - bt.out_begin) != cudaSuccess)
     return cuda_fail(cudaErrorMemoryAllocation, "pinned staging", __FILE__, __LINE__);
+  const int64_t t_pinned = now_ns();
   char* hp = static_cast<char*>(sl.in.p);
   for (auto& g : bt.groups) {
     switch (g.kind) {
@@ -679,6 +683,7 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   }
   bt.d_buf = sl.arena;
   char* dp = static_cast<char*>(bt.d_buf);
+  const int64_t t_arena = now_ns();
   RST_CUDA(cudaMemcpyAsync(dp, hp, bt.in_bytes, cudaMemcpyHostToDevice, st));
   for (auto& g : bt.groups) {
     switch (g.kind) {
@@ -759,6 +764,19 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   RST_CUDA(cudaMemcpyAsync(sl.out.p, dp + bt.out_begin, bt.out_end - bt.out_begin,
                            cudaMemcpyDeviceToHost, st));
   RST_CUDA(cudaEventRecord(sl.ev, st));
+  // RESET_SERVER_TRACE=<ms>: report launches slower than that, by phase
+  static const double trace_ms = [] {
+    const char* v = std::getenv("RESET_SERVER_TRACE");
+    return v ? std::atof(v) : -1.0;
+  }();
+  const int64_t t_end = now_ns();
+  if (trace_ms >= 0 && (t_end - bt.t_launch) / 1e6 > trace_ms)
+    std::fprintf(stderr,
+                 "reset_server: batch %lld (%zu requests, %zu device bytes, %s) launched in "
+                 "%.3f ms: plan %.3f, pinned staging %.3f, arena %.3f, copies + kernels %.3f\n",
+                 (long long)bt.id, bt.reqs.size(), bt.d_bytes, bt.heavy ? "heavy" : "light",
+                 (t_end - bt.t_launch) / 1e6, (t_plan - bt.t_launch) / 1e6,
+                 (t_pinned - t_plan) / 1e6, (t_arena - t_pinned) / 1e6, (t_end - t_arena) / 1e6);
   return RESET_OK;
 }
 

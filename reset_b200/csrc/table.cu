@@ -43,6 +43,8 @@ constexpr bool kTileDynamic = true;  // warps take a tile's larger sets from a c
 constexpr int kThreadSetMax = 8;      // sets with deg <= this: thread per set
 constexpr int kTileSmemBudget = 72 * 1024;
 constexpr int kBigFillSmemMax = 64 * 1024;  // buckets whose fill bytes fit smem
+constexpr int kHugeKeys = 1 << 16;  // sets this long get the parallel build
+constexpr int kMaxHuge = 64;        // ... at most this many per table
 
 struct Geom {
   int R_max;  // buckets per shared-memory tile (stride of a slot plane)
@@ -93,8 +95,9 @@ __global__ void meta_kernel(const int32_t* __restrict__ off, int32_t n,
                             float alpha, int b, int LT,
                             int32_t* __restrict__ len,
                             int64_t* __restrict__ len64,
-                            int32_t* __restrict__ info,  // [0]=max_len [1]=big
+                            int32_t* __restrict__ info,  // [0]=max_len [1]=big [2]=huge
                             int32_t* __restrict__ big_list,
+                            int32_t* __restrict__ huge_list,
                             int32_t* __restrict__ status) {
   int mx = 0;
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n;
@@ -108,7 +111,15 @@ __global__ void meta_kernel(const int32_t* __restrict__ off, int32_t n,
     len[u] = l;
     len64[u] = l;
     mx = max(mx, l);
-    if (l > LT) big_list[atomicAdd(&info[1], 1)] = (int32_t)u;
+    if (l > LT) {
+      // sets of kHugeKeys or more keys (up to kMaxHuge of them) get the
+      // parallel build; the rest of the long sets one warp each
+      int slot = d >= kHugeKeys ? atomicAdd(&info[2], 1) : kMaxHuge;
+      if (slot < kMaxHuge)
+        huge_list[slot] = (int32_t)u;
+      else
+        big_list[atomicAdd(&info[1], 1)] = (int32_t)u;
+    }
   }
   mx = __reduce_max_sync(kFull, mx);
   if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(&info[0], mx);
@@ -497,6 +508,187 @@ __global__ void __launch_bounds__(kThreads)
     });
 }
 
+// ----------------------------------------------------------- huge build --
+//
+// One set of d >= kHugeKeys keys, built in parallel with exactly the slots
+// of sequential CSR-order insertion:
+//  1. home bucket of every key, keys per home bucket (cnt);
+//  2. the final fills: in linear probing they do not depend on the
+//     insertion order -- the keys carried from bucket h to h+1 are
+//     c(h+1) = max(0, c(h) + cnt(h) - b), a max-plus recurrence solved by
+//     one scan (c -> max(P, c + Q) composes); the table is circular and
+//     holds fewer keys than slots, so the carry into bucket 0 is the P of
+//     the whole composition;
+//  3. clusters = runs of buckets a carry flows through (a bucket with carry
+//     0 starts one); keys never leave their home bucket's cluster;
+//  4. keys stably sorted by cluster (so CSR order within each), then one
+//     thread per cluster replays the sequential rule on its keys.
+
+struct CarryFn {  // c -> max(p, c + q)
+  long long p, q;
+};
+struct ComposeCarry {  // apply a, then b
+  __host__ __device__ CarryFn operator()(const CarryFn& a, const CarryFn& b) const {
+    return CarryFn{max(b.p, a.p + b.q), a.q + b.q};
+  }
+};
+struct MaxI32 {
+  __host__ __device__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
+
+template <bool HIER>
+__global__ void huge_home_kernel(const int32_t* __restrict__ keys, int64_t d, int lg,
+                                 int lg_max, int32_t* __restrict__ home,
+                                 int32_t* __restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int h = home_bucket<HIER>(__ldg(keys + i), lg, lg_max);
+    home[i] = h;
+    atomicAdd(cnt + h, 1);
+  }
+}
+
+__global__ void huge_fn_kernel(const int32_t* __restrict__ cnt, int64_t l, int b,
+                               CarryFn* __restrict__ fn) {
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < l;
+       h += (int64_t)gridDim.x * blockDim.x)
+    fn[h] = CarryFn{0, (long long)cnt[h] - b};
+}
+
+// start[h] = h where the carry into bucket h is 0, else -1 (fn holds the
+// inclusive prefix compositions).
+__global__ void huge_start_kernel(const CarryFn* __restrict__ fn, int64_t l,
+                                  int32_t* __restrict__ start) {
+  const long long c0 = fn[l - 1].p;
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < l;
+       h += (int64_t)gridDim.x * blockDim.x) {
+    const long long c = h == 0 ? c0 : max(fn[h - 1].p, c0 + fn[h - 1].q);
+    start[h] = c == 0 ? (int32_t)h : -1;
+  }
+}
+
+// Cluster of every key: the last carry-free bucket at or before its home
+// (before bucket 0: the last one of the table, the cluster that wraps).
+__global__ void huge_cluster_kernel(const int32_t* __restrict__ home, int64_t d,
+                                    const int32_t* __restrict__ cstart, int64_t l,
+                                    int32_t* __restrict__ cid, int32_t* __restrict__ idx) {
+  const int32_t wrap = cstart[l - 1];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = cstart[home[i]];
+    cid[i] = c >= 0 ? c : wrap;
+    idx[i] = (int32_t)i;
+  }
+}
+
+// One thread per cluster: its keys (sorted_idx[seg .. seg + len), CSR
+// order) inserted by the sequential rule; fill[] starts at 0.
+__global__ void huge_place_kernel(const int32_t* __restrict__ keys,
+                                  const int32_t* __restrict__ home,
+                                  const int32_t* __restrict__ sorted_idx,
+                                  const int32_t* __restrict__ run_len,
+                                  const int32_t* __restrict__ run_off,
+                                  const int32_t* __restrict__ n_runs, int64_t l, int b,
+                                  int64_t bn, int32_t* __restrict__ fill,
+                                  int32_t* __restrict__ G, int32_t* __restrict__ status) {
+  const int64_t nr = *n_runs;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nr;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t s0 = run_off[r], s1 = s0 + run_len[r];
+    for (int32_t j = s0; j < s1; ++j) {
+      const int32_t i = sorted_idx[j];
+      int64_t h = home[i];
+      int64_t guard = 0;
+      while (fill[h] >= b && guard < l) {
+        h = (h + 1) & (l - 1);
+        ++guard;
+      }
+      if (guard >= l) {
+        atomicOr(status, kErrTableFull);
+        continue;
+      }
+      const int k = fill[h]++;
+      G[h + (int64_t)k * bn] = keys[i];
+    }
+  }
+}
+
+// A huge set's rows in bucket order: its non-empty slots in (bucket, slot)
+// order, compacted.  Block k covers indices [k*kHugeChunk, (k+1)*kHugeChunk)
+// of the l*b (bucket, slot) pairs, each warp a contiguous span of them.
+constexpr int kHugeChunk = 8192;
+
+__device__ __forceinline__ int32_t huge_slot(const int32_t* G, int64_t bn, int b, int64_t i) {
+  return b == 1 ? G[i] : G[i / b + (i % b) * bn];
+}
+
+__device__ __forceinline__ int huge_warp_count(const int32_t* G, int64_t bn, int b,
+                                               int64_t lo, int64_t hi) {
+  const int lane = threadIdx.x & 31;
+  int c = 0;
+  for (int64_t i0 = lo; i0 < hi; i0 += 32) {
+    const int64_t i = i0 + lane;
+    c += __popc(__ballot_sync(kFull, i < hi && huge_slot(G, bn, b, i) != -1));
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    huge_count_kernel(const int32_t* __restrict__ G, int64_t bn, int b, int64_t total,
+                      int32_t* __restrict__ blk_cnt) {
+  __shared__ int s_c[kWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = (int64_t)blockIdx.x * kHugeChunk;
+  const int span = kHugeChunk / kWarps;
+  const int64_t lo = min(total, base + (int64_t)warp * span), hi = min(total, lo + span);
+  const int c = huge_warp_count(G, bn, b, lo, hi);
+  if (lane == 0) s_c[warp] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kWarps; ++w) t += s_c[w];
+    blk_cnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    huge_write_kernel(const int32_t* __restrict__ G, int64_t bn, int b, int64_t total,
+                      const int32_t* __restrict__ blk_off, int32_t* __restrict__ out) {
+  __shared__ int s_c[kWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = (int64_t)blockIdx.x * kHugeChunk;
+  const int span = kHugeChunk / kWarps;
+  const int64_t lo = min(total, base + (int64_t)warp * span), hi = min(total, lo + span);
+  const int c = huge_warp_count(G, bn, b, lo, hi);
+  if (lane == 0) s_c[warp] = c;
+  __syncthreads();
+  int64_t w = blk_off[blockIdx.x];
+  for (int k = 0; k < warp; ++k) w += s_c[k];
+  const unsigned lt = lanemask_lt();
+  for (int64_t i0 = lo; i0 < hi; i0 += 32) {
+    const int64_t i = i0 + lane;
+    const int32_t v = i < hi ? huge_slot(G, bn, b, i) : -1;
+    const unsigned msk = __ballot_sync(kFull, v != -1);
+    if (v != -1) out[w + __popc(msk & lt)] = v;
+    w += __popc(msk);
+  }
+}
+
+// (row start, keys, table length, table offset) of each huge set.
+__global__ void huge_info_kernel(const int32_t* __restrict__ off,
+                                 const int32_t* __restrict__ len,
+                                 const int64_t* __restrict__ off64,
+                                 const int32_t* __restrict__ huge_list, int nh,
+                                 int64_t* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nh) return;
+  const int u = huge_list[k];
+  out[4 * k + 0] = off[u];
+  out[4 * k + 1] = (int64_t)off[u + 1] - off[u];
+  out[4 * k + 2] = len[u];
+  out[4 * k + 3] = off64[u];
+}
+
 // ------------------------------------------------- standalone extraction --
 
 __global__ void __launch_bounds__(kThreads)
@@ -622,6 +814,113 @@ void destroy(reset_table* t) {
   delete t;
 }
 
+// The parallel build of one huge set (see huge_home_kernel): row start rs,
+// d keys, table length l (a power of two) at offset toff.  Scratch comes
+// from the table pool, stream-ordered; no host synchronisation.
+template <bool HIER>
+reset_status build_huge(const reset_table* t, const int32_t* d_elems, int64_t rs, int64_t d,
+                        int64_t l, int64_t toff, int32_t* d_hash_out, cudaStream_t st) {
+  const int b = t->bucket;
+  const int64_t bn = t->bucket_num;
+  const int lg = 63 - __builtin_clzll((unsigned long long)l);
+  int32_t* G = t->d_table + toff;
+  for (int k = 0; k < b; ++k)
+    RST_CUDA(cudaMemsetAsync(G + (int64_t)k * bn, 0xFF, sizeof(int32_t) * (size_t)l, st));
+  if (d <= 0) return RESET_OK;
+  const int di = (int)d, li = (int)l;
+  const int64_t total = l * b;
+  const int64_t nblk = (total + kHugeChunk - 1) / kHugeChunk;
+  const int32_t* keys = d_elems + rs;
+  // CUB temporary sizes
+  size_t tb[6] = {0, 0, 0, 0, 0, 0};
+  CarryFn* nf = nullptr;
+  int32_t* ni = nullptr;
+  RST_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tb[0], nf, nf, ComposeCarry(), li, st));
+  RST_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tb[1], ni, ni, MaxI32(), li, st));
+  RST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb[2], ni, ni, ni, ni, di, 0,
+                                           std::max(lg, 1), st));
+  RST_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, tb[3], ni, ni, ni, ni, di, st));
+  RST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb[4], ni, ni, di, st));
+  RST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb[5], ni, ni, (int)nblk, st));
+  size_t tmp = 0;
+  for (size_t x : tb) tmp = std::max(tmp, x);
+  // one scratch block: 8 arrays of d ints, 4 of l ints, l carry functions
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t sd = al(4 * (size_t)d), sl = al(4 * (size_t)l);
+  const size_t bytes = 8 * sd + 4 * sl + al(sizeof(CarryFn) * (size_t)l) +
+                       2 * al(4 * (size_t)(nblk + 1)) + al(16) + al(tmp);
+  char* base = nullptr;
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&base), bytes, st));
+  char* q = base;
+  auto carve = [&q](size_t n) {
+    char* r = q;
+    q += n;
+    return r;
+  };
+  int32_t* home = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* cid = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* idx = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* cid_s = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* idx_s = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* runs = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* run_len = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* run_off = reinterpret_cast<int32_t*>(carve(sd));
+  int32_t* cnt = reinterpret_cast<int32_t*>(carve(sl));
+  int32_t* start = reinterpret_cast<int32_t*>(carve(sl));
+  int32_t* cstart = reinterpret_cast<int32_t*>(carve(sl));
+  int32_t* fill = reinterpret_cast<int32_t*>(carve(sl));
+  CarryFn* fn = reinterpret_cast<CarryFn*>(carve(al(sizeof(CarryFn) * (size_t)l)));
+  int32_t* blk = reinterpret_cast<int32_t*>(carve(al(4 * (size_t)(nblk + 1))));
+  int32_t* blk_off = reinterpret_cast<int32_t*>(carve(al(4 * (size_t)(nblk + 1))));
+  int32_t* n_runs = reinterpret_cast<int32_t*>(carve(al(16)));
+  void* ctmp = carve(al(tmp));
+
+  reset_status rs_out = RESET_OK;
+  auto run = [&]() -> reset_status {
+    RST_CUDA(cudaMemsetAsync(cnt, 0, 4 * (size_t)l, st));
+    RST_CUDA(cudaMemsetAsync(fill, 0, 4 * (size_t)l, st));
+    note_launch();
+    huge_home_kernel<HIER><<<grid_for(d, kThreads), kThreads, 0, st>>>(keys, d, lg, t->lg_max,
+                                                                      home, cnt);
+    note_launch();
+    huge_fn_kernel<<<grid_for(l, kThreads), kThreads, 0, st>>>(cnt, l, b, fn);
+    size_t x = tmp;
+    RST_CUDA(cub::DeviceScan::InclusiveScan(ctmp, x, fn, fn, ComposeCarry(), li, st));
+    note_launch();
+    huge_start_kernel<<<grid_for(l, kThreads), kThreads, 0, st>>>(fn, l, start);
+    x = tmp;
+    RST_CUDA(cub::DeviceScan::InclusiveScan(ctmp, x, start, cstart, MaxI32(), li, st));
+    note_launch();
+    huge_cluster_kernel<<<grid_for(d, kThreads), kThreads, 0, st>>>(home, d, cstart, l, cid,
+                                                                    idx);
+    x = tmp;
+    RST_CUDA(cub::DeviceRadixSort::SortPairs(ctmp, x, cid, cid_s, idx, idx_s, di, 0,
+                                             std::max(lg, 1), st));
+    x = tmp;
+    RST_CUDA(cub::DeviceRunLengthEncode::Encode(ctmp, x, cid_s, runs, run_len, n_runs, di, st));
+    x = tmp;
+    RST_CUDA(cub::DeviceScan::ExclusiveSum(ctmp, x, run_len, run_off, di, st));
+    note_launch();
+    huge_place_kernel<<<grid_for(d, kThreads), kThreads, 0, st>>>(
+        keys, home, idx_s, run_len, run_off, n_runs, l, b, bn, fill, G, t->d_status);
+    RST_CUDA(cudaGetLastError());
+    if (d_hash_out) {
+      note_launch();
+      huge_count_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(G, bn, b, total, blk);
+      x = tmp;
+      RST_CUDA(cub::DeviceScan::ExclusiveSum(ctmp, x, blk, blk_off, (int)nblk, st));
+      note_launch();
+      huge_write_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(G, bn, b, total, blk_off,
+                                                             d_hash_out + rs);
+      RST_CUDA(cudaGetLastError());
+    }
+    return RESET_OK;
+  };
+  rs_out = run();
+  cudaFreeAsync(base, st);
+  return rs_out;
+}
+
 template <bool HIER>
 reset_status launch_builds(const reset_table* t, const int32_t* d_off,
                            const int32_t* d_elems, const int32_t* d_tile_first,
@@ -684,6 +983,8 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
 
   int32_t* d_info = nullptr;
   int32_t* d_big = nullptr;
+  int32_t* d_huge = nullptr;
+  int64_t* d_huge_info = nullptr;
   int32_t* d_tile_first = nullptr;
   int64_t* d_bn = nullptr;
   void* d_tmp = nullptr;
@@ -692,6 +993,8 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
     cudaStreamSynchronize(st);
     if (d_info) cudaFreeAsync(d_info, st);
     if (d_big) cudaFreeAsync(d_big, st);
+    if (d_huge) cudaFreeAsync(d_huge, st);
+    if (d_huge_info) cudaFreeAsync(d_huge_info, st);
     if (d_tile_first) cudaFreeAsync(d_tile_first, st);
     if (d_bn) cudaFreeAsync(d_bn, st);
     if (d_tmp) cudaFreeAsync(d_tmp, st);
@@ -720,11 +1023,12 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   POOL_ALLOC(d_bn, sizeof(int64_t));
   BUILD_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int32_t) * 4, st));
   POOL_ALLOC(d_big, sizeof(int32_t) * (n > 0 ? n : 1));
+  POOL_ALLOC(d_huge, sizeof(int32_t) * kMaxHuge);
 
   if (n > 0) {
     note_launch(); meta_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_off, n, p.alpha, p.bucket,
                                                    g.LT, t->d_len, t->d_off64,
-                                                   d_info, d_big, t->d_status);
+                                                   d_info, d_big, d_huge, t->d_status);
     BUILD_CUDA(cudaGetLastError());
     size_t tmp_bytes = 0;
     BUILD_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, t->d_off64,
@@ -744,7 +1048,20 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
   t->max_len = n > 0 ? info[0] : 8;
   t->lg_max = 31 - __builtin_clz((unsigned)t->max_len);
   const int32_t n_big = info[1];
+  const int n_huge = std::min(info[2], kMaxHuge);
   if (bn >= ((int64_t)1 << 56)) return fail(arg_fail("table too large"));
+  // huge sets: their rows and table places on the host (one more sync,
+  // only for tables that have such sets)
+  int64_t huge[4 * kMaxHuge];
+  if (n_huge > 0) {
+    POOL_ALLOC(d_huge_info, sizeof(int64_t) * 4 * kMaxHuge);
+    note_launch(); huge_info_kernel<<<1, kMaxHuge, 0, st>>>(d_off, t->d_len, t->d_off64,
+                                                            d_huge, n_huge, d_huge_info);
+    BUILD_CUDA(cudaGetLastError());
+    BUILD_CUDA(cudaMemcpyAsync(huge, d_huge_info, sizeof(int64_t) * 4 * n_huge,
+                               cudaMemcpyDeviceToHost, st));
+    BUILD_CUDA(cudaStreamSynchronize(st));
+  }
 
   size_t tbytes = sizeof(int32_t) * (size_t)bn * p.bucket;
   POOL_ALLOC(t->d_table, tbytes > 0 ? tbytes : 16);
@@ -767,9 +1084,17 @@ reset_status reset_table_build(const int32_t* d_off, const int32_t* d_elems,
       rs = launch_builds<false>(t, d_off, d_elems, d_tile_first, n_tiles,
                                 d_big, n_big, g, d_hash_out, st);
     if (rs != RESET_OK) return fail(rs);
+    for (int k = 0; k < n_huge && rs == RESET_OK; ++k) {
+      const int64_t* h = huge + 4 * k;
+      rs = t->hier ? build_huge<true>(t, d_elems, h[0], h[1], h[2], h[3], d_hash_out, st)
+                   : build_huge<false>(t, d_elems, h[0], h[1], h[2], h[3], d_hash_out, st);
+    }
+    if (rs != RESET_OK) return fail(rs);
   }
   cudaFreeAsync(d_info, st);
   cudaFreeAsync(d_big, st);
+  cudaFreeAsync(d_huge, st);
+  if (d_huge_info) cudaFreeAsync(d_huge_info, st);
   cudaFreeAsync(d_tile_first, st);
   cudaFreeAsync(d_bn, st);
   if (d_tmp) cudaFreeAsync(d_tmp, st);

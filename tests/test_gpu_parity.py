@@ -64,6 +64,28 @@ def _check_table(R, cuda, O, off, elems, alpha, bucket, hier):
 
 
 @pytest.mark.parametrize("hier", [True, False])
+@pytest.mark.parametrize("alpha,bucket", [(1.0, 1), (0.9, 2), (0.2, 5)])
+def test_table_layout_huge_sets(R, cuda, oracle_mod, hier, alpha, bucket):
+    """Sets of 2^16 keys and more are built in parallel (final fills by a
+    scan, clusters replayed in CSR order) and must equal sequential CSR-order
+    insertion byte for byte: dense tables (long clusters), repeated keys,
+    keys crowding the last buckets (a cluster that wraps to bucket 0), and
+    small sets around them."""
+    rng = np.random.default_rng(11)
+    big = rng.integers(0, 1 << 24, 70000)
+    big[:3000] = big[0]                                   # one key repeated
+    big[3000:6000] = (1 << 20) - 1 - rng.integers(0, 4, 3000)  # high buckets
+    rng.shuffle(big)
+    other = rng.integers(0, 1 << 20, 80000)
+    rows = [np.sort(rng.choice(1 << 20, 40, replace=False)), big, other,
+            np.zeros(0, np.int64), np.sort(rng.choice(1 << 20, 300, replace=False))]
+    off = np.zeros(len(rows) + 1, np.int32)
+    off[1:] = np.cumsum([r.size for r in rows])
+    elems = np.concatenate(rows).astype(np.int32)
+    _check_table(R, cuda, oracle_mod, off, elems, alpha, bucket, hier)
+
+
+@pytest.mark.parametrize("hier", [True, False])
 @pytest.mark.parametrize("alpha,bucket", [(0.2, 5), (0.5, 3), (1.0, 1), (0.1, 9), (0.25, 4)])
 def test_table_layout_rmat(R, cuda, oracle_mod, hier, alpha, bucket):
     off, cols = oracle_mod.rmat_graph(12, 16, 0x5EED0012, oriented=False)
