@@ -255,24 +255,32 @@ def sss_join_ours(a, rank, world, local):
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = _sss_cpu(off.cpu().numpy(), tok.cpu().numpy(),
-                                        pa.cpu().numpy(), pb.cpu().numpy(), a.cpu_seconds)
+                                        pa.cpu().numpy(), pb.cpu().numpy(), a.cpu_seconds,
+                                        bt.flags[:P].cpu().numpy())
+        line["config"]["pairs_checked_exactly"] = line["cpu_baseline"].pop("checked")
     bt.close()
     _finish(line, rank, world)
 
 
-def _sss_cpu(off, tok, pa, pb, seconds):
-    """Oracle hash-probe decisions (one thread) on a bounded sample."""
+def _sss_cpu(off, tok, pa, pb, seconds, flags=None):
+    """Oracle hash-probe decisions (one thread) on a bounded sample; with
+    the GPU's decisions of the same candidates, every sampled one must be
+    equal (returned as "checked")."""
     import oracle
     ot = oracle.Table(off, tok, hier=1)
     done, chunk = 0, 20000
     t0 = time.perf_counter()
     while done < pa.size and time.perf_counter() - t0 < seconds:
-        oracle.sss(ot, pa[done:done + chunk], pb[done:done + chunk], mode=1, num=7, den=10)
+        f, _ = oracle.sss(ot, pa[done:done + chunk], pb[done:done + chunk], mode=1,
+                          num=7, den=10)
+        if flags is not None:
+            assert np.array_equal(f, flags[done:done + f.size]), "self-join decision differs"
         done += min(chunk, pa.size - done)
     el = time.perf_counter() - t0
     return {"value": done / el, "unit": "intersections/s", "cores": 1, "kind": "port",
             "sample": f"first {done} candidate pairs decided by the oracle's hash probe "
-                      f"in {el:.1f} s (table build not timed)"}
+                      f"in {el:.1f} s (table build not timed)",
+            "checked": done if flags is not None else 0}
 
 
 # ================================================================ serving ==
@@ -404,6 +412,48 @@ def _serve_report(srv_factory, reqs, submit, a, rng, check):
     return cap, lat_cap, stats_cap, sweep, per_call
 
 
+def _ir_roofline(torch, api, t, toff, docs, h_toff, h_docs, qs):
+    """The IR kernels' roofline on one reset_ir call over the queries `qs`
+    (the kernels the served batches run: slice probe, slice scan, gather).
+    Algorithmic bytes per query: 4 per candidate of the first list, 4 per
+    probe (a candidate still alive at a further term reads one slot), 4
+    per survivor written; the alive candidates come from exact host
+    intersections."""
+    qlist = np.concatenate(qs).astype(np.int32)
+    qoff = np.zeros(len(qs) + 1, np.int32)
+    qoff[1:] = np.cumsum([q.size for q in qs])
+    dq = torch.from_numpy(qlist).cuda()
+    dqo = torch.from_numpy(qoff).cuda()
+    alg = 0
+    for q in qs:
+        alive = h_docs[h_toff[q[0]]:h_toff[q[0] + 1]]
+        alg += 4 * alive.size
+        for term in q[1:]:
+            alg += 4 * alive.size
+            alive = np.intersect1d(alive, h_docs[h_toff[term]:h_toff[term + 1]],
+                                   assume_unique=True)
+        alg += 4 * alive.size
+    st = torch.cuda.current_stream()
+    api.ir(t, toff, docs, dq, dqo)
+    ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        api.ir(t, toff, docs, dq, dqo)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    best = min(ms)
+    peak, src = _peak()
+    achieved = alg / (best / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "ir_slice_kernel + slice scan + gather",
+            "timed": f"one reset_ir call over {len(qs)} queries of the stream "
+                     "(CUDA events on its stream; includes its host-side sizing read)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": src, "traffic": None,
+            "algorithmic_bytes_per_launch": int(alg), "ms_per_launch": best}
+
+
 def ir_serve_ours(a, rank, world, local):
     torch = _setup(local, world)
     from reset_b200 import api, _lib
@@ -444,6 +494,7 @@ def ir_serve_ours(a, rank, world, local):
         cap, lat_cap, st, sweep, per_call = _serve_report(factory, reqs, submit, a, rng, check)
     launches = L.reset_kernel_launches() - l0
     (cap,) = _maxr([cap], world)
+    roof = _ir_roofline(torch, api, t, toff, docs, h_toff, h_docs, reqs[:512])
     qterms = sum(q.size for q in reqs) / len(reqs)
     res_ints = sum(int(df[q[0]]) for q in reqs) / len(reqs)
     line = {
@@ -472,7 +523,7 @@ def ir_serve_ours(a, rank, world, local):
                 "note": "serving is end to end by construction: host query arrays in, "
                         "host result lists out, through reset_server_*; d2h is an upper "
                         "bound (first-term lengths; only survivors are copied)"},
-        "roofline": None,
+        "roofline": roof,
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -805,6 +856,7 @@ def run_reference(a, rank, world):
         pa = rng.integers(0, n, 400_000).astype(np.int32)
         pb = rng.integers(0, n, 400_000).astype(np.int32)
         cb = _sss_cpu(off, tok, pa, pb, a.cpu_seconds)
+        cb.pop("checked")
         unit, metric = "intersections/s", "set-intersections/sec (Jaccard 0.7 decisions)"
     elif a.workload == "ir-serve":
         rng = np.random.default_rng(SEED_IR)
