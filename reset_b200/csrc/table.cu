@@ -44,7 +44,7 @@ constexpr int kThreadSetMax = 8;      // sets with deg <= this: thread per set
 constexpr int kTileSmemBudget = 72 * 1024;
 constexpr int kBigFillSmemMax = 64 * 1024;  // buckets whose fill bytes fit smem
 constexpr int kHugeKeys = 1 << 16;  // sets this long get the parallel build
-constexpr int kMaxHuge = 64;        // ... at most this many per table
+constexpr int kMaxHuge = 512;       // ... at most this many per table
 
 struct Geom {
   int R_max;  // buckets per shared-memory tile (stride of a slot plane)
