@@ -256,10 +256,14 @@ __device__ void insert_set_warp(const int32_t* __restrict__ keys, int d,
   const int lane = threadIdx.x & 31;
   const int l = 1 << lg;
   const unsigned lt = lanemask_lt(), gt = lanemask_gt();
+  // the next round's keys are loaded before this round is inserted, so the
+  // load latency overlaps the insertion (long sets take many rounds)
+  int xn = lane < d ? __ldg(keys + lane) : 0;
   for (int j0 = 0; j0 < d; j0 += 32) {
     const int j = j0 + lane;
     const bool valid = j < d;
-    const int x = valid ? __ldg(keys + j) : 0;
+    const int x = xn;
+    if (j + 32 < d) xn = __ldg(keys + j + 32);
     int h = valid ? home_bucket<HIER>(x, lg, lg_max) : 0;
     unsigned pending = __ballot_sync(kFull, valid);
     while (pending) {
