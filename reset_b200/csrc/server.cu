@@ -467,6 +467,12 @@ bool trivially_empty(const Req& r) {
 
 // Groups, lays out, fills the pinned input, allocates, copies in, launches,
 // copies out and records the slot's event.
+LeaseP take_lease(reset_server* s, size_t bytes);
+
+// IR batches whose survivors can take at most this many bytes bring them
+// back with the small outputs (one round trip instead of two).
+constexpr size_t kOnePhaseBytes = size_t(1) << 20;
+
 reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
   const int64_t slice = ir_slice_size();
   // ---- groups
@@ -759,6 +765,29 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
         RST_CUDA(cudaGetLastError());
         break;
       }
+    }
+  }
+  // Small IR batches: copy each group's whole survivor region (bounded by
+  // the first terms' lengths) into an arena range now, so the batch
+  // completes in one phase; larger ones copy only the survivors once their
+  // number is known (enqueue_results).
+  size_t ir_bound = 0;
+  for (auto& g : bt.groups)
+    if (g.kind == RESET_REQ_IR) ir_bound += 4 * (size_t)g.aux;
+  if (ir_bound > 0 && ir_bound <= kOnePhaseBytes) {
+    if (LeaseP lease = take_lease(s, ir_bound)) {
+      size_t at = 0;
+      for (auto& g : bt.groups) {
+        if (g.kind != RESET_REQ_IR) continue;
+        g.dense_host = at / 4;
+        if (g.aux > 0)
+          RST_CUDA(cudaMemcpyAsync(lease->p + at, dp + g.sc[2], 4 * (size_t)g.aux,
+                                   cudaMemcpyDeviceToHost, st));
+        at += 4 * (size_t)g.aux;
+      }
+      bt.res_ptr = reinterpret_cast<const int32_t*>(lease->p);
+      bt.res = std::move(lease);
+      bt.phase = 1;
     }
   }
   RST_CUDA(cudaMemcpyAsync(sl.out.p, dp + bt.out_begin, bt.out_end - bt.out_begin,
