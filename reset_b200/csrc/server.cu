@@ -683,7 +683,7 @@ reset_status launch_batch(reset_server* s, Slot& sl, Batch& bt) {
     if (sl.arena) RST_CUDA(cudaFreeAsync(sl.arena, st));
     sl.arena = nullptr;
     sl.arena_cap = 0;
-    const size_t cap = std::max(bt.d_bytes, (size_t)(1u << 20));
+    const size_t cap = std::max(bt.d_bytes + bt.d_bytes / 4, (size_t)(1u << 20));
     RST_CUDA(cudaMallocFromPoolAsync(&sl.arena, cap, s->pool, st));
     sl.arena_cap = cap;
   }
@@ -1183,7 +1183,30 @@ reset_status reset_server_add_index(reset_server* s, const reset_table* t,
     return RESET_ERR_OOM;
   }
   RST_CUDA(cudaMemcpy(ix.h_off.data(), d_off, 4 * ((size_t)t->n + 1), cudaMemcpyDeviceToHost));
+  // Device bytes of the largest single request on this index (an IR query
+  // of up to six terms whose first list is the longest set).  Slot arenas
+  // are grown to it now: growing one while serving maps new pool memory in
+  // the scheduler thread, which stalled every arrival behind a heavy
+  // request by 20-60 ms.
+  int64_t max_len = 0;
+  for (int32_t u = 0; u < t->n; ++u)
+    max_len = std::max<int64_t>(max_len, ix.h_off[u + 1] - ix.h_off[u]);
+  const int64_t slice = ir_slice_size();
+  const size_t need = (size_t)(4 * 6 + 32 + 4 * max_len +
+                               (4 * slice + 12) * ((max_len + slice - 1) / slice)) +
+                      (size_t(1) << 16);
   std::lock_guard<std::mutex> lk(s->mu);
+  if (s->inflight == 0) {  // slots idle: grow their arenas (stream-ordered, then waited for)
+    for (auto& sl : s->slots) {
+      if (sl.busy || sl.arena_cap >= need) continue;
+      if (sl.arena) RST_CUDA(cudaFreeAsync(sl.arena, sl.st));
+      sl.arena = nullptr;
+      sl.arena_cap = 0;
+      RST_CUDA(cudaMallocFromPoolAsync(&sl.arena, need, s->pool, sl.st));
+      RST_CUDA(cudaStreamSynchronize(sl.st));
+      sl.arena_cap = need;
+    }
+  }
   s->indexes.push_back(std::move(ix));
   *index_out = (int32_t)s->indexes.size() - 1;
   return RESET_OK;
