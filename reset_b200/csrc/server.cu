@@ -445,7 +445,9 @@ reset_status plan_request(const reset_server* s, Req* r) {
         if (x < 0) return arg_fail("raw keys must be >= 0");
       r->aux = calc_len((int)nb, 0.2f, 5);
       r->dev_bytes = 4 * (int64_t)(r->a.size() + nb) + 20 * r->aux + 16;
-      r->cost = (int64_t)r->a.size() + nb;
+      // B's table is cleared (5 slots per bucket) and built (an atomic
+      // insertion per key) before A probes it: a large pair is heavy work
+      r->cost = (int64_t)r->a.size() + 4 * nb + 5 * r->aux;
       break;
     }
     default:
