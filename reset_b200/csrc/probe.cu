@@ -565,7 +565,7 @@ reset_status reset_tc_count_ex(const reset_table* t, const int32_t* d_off,
   const bool cols16 = (reinterpret_cast<uintptr_t>(d_cols) & 15) == 0;
   if (method == 3 && !cols16)
     return arg_fail("method 3 needs a 16-byte aligned column array");
-  if (method == 0) method = cols16 && m <= INT32_MAX - 4 ? 3 : 1;
+  if (method == 0) method = cols16 && m <= INT32_MAX - 16 ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;

@@ -256,21 +256,26 @@ __device__ __forceinline__ int owner_lane_n(int P, int f) {
 //
 // PF: the next R chunks of keys are loaded before the current ones are
 // probed (software pipelining across rounds).
+//
+// CW: keys per lane and round (4: one 16-byte load; 8: two, so the row
+// search and chunk bookkeeping are paid once per 8 keys).
 template <bool HIER, int R, bool PAIRS = false, int NR = 32, int QCAP = kQueue,
-          bool KEEP = false, bool PF = false>
+          bool KEEP = false, bool PF = false, int CW = 4>
 __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, int cnt,
                                                 const int32_t* __restrict__ cols, int64_t m,
                                                 const int* S, int lg, int lg_max, int b,
                                                 int32_t* status, int* qx, int* qh,
                                                 int* s_cnt = nullptr, int* nq_keep = nullptr) {
   static_assert(NR >= 1 && NR <= 32 && (NR & (NR - 1)) == 0, "NR: a power of two <= 32");
-  static_assert(QCAP >= kQueue, "the queue must hold one round");
+  static_assert(CW == 4 || CW == 8, "chunks of 4 or 8 keys");
+  static_assert(QCAP >= 32 * CW, "the queue must hold one round");
+  constexpr int kShift = CW == 8 ? 3 : 2;
   static_assert(!(KEEP && PAIRS), "a kept queue carries no rows");
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int2 e = lane < cnt ? __ldg(ent + lane) : make_int2(0, 0);
   const int64_t end = (int64_t)e.x + e.y;
-  const int nc = e.y > 0 ? (int)(((end + 3) >> 2) - (e.x >> 2)) : 0;
+  const int nc = e.y > 0 ? (int)(((end + CW - 1) >> kShift) - (e.x >> kShift)) : 0;
   int total;
   const int P = warp_excl_scan(nc, &total);
   const int L = 1 << lg;
@@ -283,7 +288,7 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   const int inc1 = b > 1 ? 0 : 1;
   const int kcont = b > 1 ? 2 : 1;
   const int4* __restrict__ cols4 = reinterpret_cast<const int4*>(cols);
-  const int64_t full4 = m >> 2;  // chunks that lie wholly inside cols
+  const int64_t full = m >> kShift;  // chunks that lie wholly inside cols
   unsigned hits = 0;
   int nq = KEEP ? *nq_keep : 0;  // queued probes (warp-uniform)
   auto walk_queue = [&]() {
@@ -307,11 +312,12 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   };
   // Loads the R chunks of rounds [base, base + 32R) of this lane: keys in
   // x (-2 outside rows), rows in kk (-1 if none).
-  auto load = [&](int base, int (&x)[R][4], int (&kk)[R]) {
+  auto load = [&](int base, int (&x)[R][CW], int (&kk)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       kk[r] = -1;
-      x[r][0] = x[r][1] = x[r][2] = x[r][3] = -2;
+#pragma unroll
+      for (int j = 0; j < CW; ++j) x[r][j] = -2;
       if (base + r * 32 < total) {  // warp-uniform
         const int f = base + r * 32 + lane;
         const int k = owner_lane_n<NR>(P, f);
@@ -320,25 +326,28 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         const int kd = __shfl_sync(kFull, e.y, k);
         if (f < total) {
           kk[r] = k;
-          // m <= 2^31 - 5 (checked on the host): 4c + 3 fits an int
-          const int c = (kb >> 2) + (f - kp);
-          const int i0 = c * 4;
+          // m <= 2^31 - 16 (checked on the host): CW*c + CW - 1 fits an int
+          const int c = (kb >> kShift) + (f - kp);
+          const int i0 = c * CW;
           const int lo = kb - i0;       // elements j < lo precede the row
           const int hi = kb + kd - i0;  // elements j >= hi follow it
-          if (c < full4) {
-            const int4 q = __ldg(cols4 + c);
-            x[r][0] = q.x;
-            x[r][1] = q.y;
-            x[r][2] = q.z;
-            x[r][3] = q.w;
+          if (c < full) {
+#pragma unroll
+            for (int v = 0; v < CW / 4; ++v) {
+              const int4 q = __ldg(cols4 + (CW / 4) * c + v);
+              x[r][4 * v + 0] = q.x;
+              x[r][4 * v + 1] = q.y;
+              x[r][4 * v + 2] = q.z;
+              x[r][4 * v + 3] = q.w;
+            }
           } else {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < CW; ++j)
               if (j >= lo && j < hi) x[r][j] = __ldg(cols + i0 + j);
           }
-          if (lo > 0 || hi < 4) {  // the first or last chunk of its row
+          if (lo > 0 || hi < CW) {  // the first or last chunk of its row
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < CW; ++j)
               if (j < lo || j >= hi) x[r][j] = -2;
           }
         }
@@ -346,13 +355,13 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
     }
   };
   // Probes the keys of rounds [base, base + 32R).
-  auto probe = [&](int base, const int (&x)[R][4], const int (&kk)[R]) {
+  auto probe = [&](int base, const int (&x)[R][CW], const int (&kk)[R]) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (base + r * 32 >= total) break;  // warp-uniform
       unsigned hr = 0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < CW; ++j) {
         const int xx = x[r][j];
         const int h = (int)(((unsigned)xx & hmask) >> hsh);
         const int s0 = S[h];
@@ -369,7 +378,7 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
         }
         nq += __popc(pm);
       }
-      if (nq > QCAP - kQueue) walk_queue();
+      if (nq > QCAP - 32 * CW) walk_queue();
       hits += hr;
       if (PAIRS) {
         const unsigned grp = __match_any_sync(kFull, kk[r]);
@@ -381,22 +390,22 @@ __device__ __forceinline__ unsigned staged_keys(const int2* __restrict__ ent, in
   if (PF) {
     // the next R chunks are loaded before this round's keys are probed,
     // so their latency hides behind the probes
-    int xn[R][4], kn[R];
+    int xn[R][CW], kn[R];
     if (total > 0) load(0, xn, kn);
     for (int base = 0; base < total; base += 32 * R) {
-      int x[R][4], kk[R];
+      int x[R][CW], kk[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         kk[r] = kn[r];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[r][j] = xn[r][j];
+        for (int j = 0; j < CW; ++j) x[r][j] = xn[r][j];
       }
       if (base + 32 * R < total) load(base + 32 * R, xn, kn);
       probe(base, x, kk);
     }
   } else {
     for (int base = 0; base < total; base += 32 * R) {
-      int x[R][4], kk[R];
+      int x[R][CW], kk[R];
       load(base, x, kk);
       probe(base, x, kk);
     }
