@@ -128,47 +128,6 @@ __global__ void __launch_bounds__(kOT)
   }
 }
 
-// Sort form of the grouping: owner (n for lanes past the end or bad ids)
-// and prober row of every edge, written in edge order for a stable radix
-// sort by owner.
-__global__ void __launch_bounds__(kOT)
-    own_key_kernel(const int32_t* __restrict__ eoff, const int32_t* __restrict__ ecols,
-                   const int32_t* __restrict__ chunk_row, const int32_t* __restrict__ koff,
-                   int32_t n, int64_t m, uint32_t* __restrict__ keys, int2* __restrict__ vals,
-                   int32_t* __restrict__ status) {
-  const int lane = threadIdx.x & 31;
-  const int64_t me = min(m, (int64_t)__ldg(eoff + n));
-  const int64_t n_chunks = (me + 31) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n_chunks;
-       c += nw) {
-    const EdgeOwner eo = edge_owner(eoff, ecols, chunk_row, koff, n, me, c, status);
-    const int64_t e = c * 32 + lane;
-    if (e < me) {
-      keys[e] = eo.ok ? (uint32_t)eo.owner : (uint32_t)n;
-      vals[e] = make_int2(eo.prober_start, eo.prober_len);
-    }
-  }
-  // keys past the CSR's own edge count (if m exceeds it) sort last
-  for (int64_t e = me + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    keys[e] = (uint32_t)n;
-    vals[e] = make_int2(0, 0);
-  }
-}
-
-// goff[w] = first index of the sorted keys with key >= w, w = 0..n: every
-// index i fills the owners between its predecessor's key and its own.
-__global__ void own_goff_kernel(const uint32_t* __restrict__ skeys, int64_t me, int32_t n,
-                                int32_t* __restrict__ goff) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= me;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t prev = i == 0 ? -1 : (int64_t)skeys[i - 1];
-    const int64_t cur = i < me ? min((int64_t)skeys[i], (int64_t)n) : (int64_t)n;
-    for (int64_t w = prev + 1; w <= cur; ++w) goff[w] = (int32_t)i;
-  }
-}
-
 // Bin of every owner with a non-empty group (see the file comment).
 // ctr[0] CTA units, ctr[1] warp owners, ctr[2] small direct owners,
 // ctr[6] direct units.
@@ -190,9 +149,6 @@ constexpr bool kOwnerPrefetch = false;
 // Keys a lane loads per round (4 or 8).  8 (two 16-byte loads) pays the row
 // search and chunk bookkeeping once per 8 keys: scale 24, b 1, 131 -> 120 ms.
 constexpr int kOwnerChunk = 8;
-// Group the edges by a radix sort of their owners (coalesced writes) instead
-// of per-edge returned atomics and scattered 8-byte writes.
-constexpr bool kSortGroups = false;
 
 template <bool HIER, int R, bool OWN = false>
 __global__ void __launch_bounds__(kOT, 2)
@@ -395,24 +351,14 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   size_t cub_bytes = 0;
   RST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (int32_t*)nullptr,
                                          (int32_t*)nullptr, (int)(n + 1), st));
-  const int end_bit = 32 - __builtin_clz((unsigned)n);  // keys 0..n
-  if (kSortGroups) {
-    size_t sb = 0;
-    RST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sb, (uint32_t*)nullptr,
-                                             (uint32_t*)nullptr, (int2*)nullptr,
-                                             (int2*)nullptr, (int)m, 0, end_bit, st));
-    cub_bytes = std::max(cub_bytes, sb);
-  }
   const int64_t max_units = n + m / kCtaSeg + 1, max_dunits = n + m / kDirSeg + 1;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t sz_cnt = al(sizeof(int32_t) * (n + 1)), sz_goff = sz_cnt;
   const size_t sz_ent = al(sizeof(int2) * m), sz_units = al(sizeof(int2) * max_units);
   const size_t sz_list = al(sizeof(int32_t) * n), sz_ctr = al(sizeof(int32_t) * 8);
   const size_t sz_dunits = al(sizeof(int2) * max_dunits);
-  // sort form: keys, sorted keys, unsorted rows
-  const size_t sz_sort = kSortGroups ? 2 * al(sizeof(uint32_t) * m) + sz_ent : 0;
   const size_t total = sz_cnt + sz_goff + sz_ent + sz_units + 2 * sz_list + sz_dunits +
-                       sz_ctr + sz_sort + al(cub_bytes);
+                       sz_ctr + al(cub_bytes);
   char* base = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&base), total, st));
   char* p = base;
@@ -424,14 +370,6 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   int32_t* dlist = reinterpret_cast<int32_t*>(p); p += sz_list;
   int2* dunits = reinterpret_cast<int2*>(p); p += sz_dunits;
   int32_t* ctr = reinterpret_cast<int32_t*>(p); p += sz_ctr;
-  uint32_t* keys = nullptr;
-  uint32_t* skeys = nullptr;
-  int2* vals = nullptr;
-  if (kSortGroups) {
-    keys = reinterpret_cast<uint32_t*>(p); p += al(sizeof(uint32_t) * m);
-    skeys = reinterpret_cast<uint32_t*>(p); p += al(sizeof(uint32_t) * m);
-    vals = reinterpret_cast<int2*>(p); p += sz_ent;
-  }
   void* cub_tmp = p;
 
   cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (n + 1), st);
@@ -439,39 +377,19 @@ reset_status tc_owner(const reset_table* t, const int4* kdesc, const int32_t* ko
   const int sms = sm_count();
   const int64_t chunks = (m + 31) / 32;
   const int g_edges = grid_stride_blocks((chunks + kOW - 1) / kOW, sms * 8);
-  if (kSortGroups) {
-    // owner keys + prober rows in edge order, a stable radix sort by owner,
-    // group offsets from the sorted keys: every write coalesced
-    if (e == cudaSuccess) {
-      note_launch();
-      own_key_kernel<<<g_edges, kOT, 0, st>>>(eoff, ecols, echunk_rows, koff, t->n, me, keys,
-                                              vals, t->d_status);
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess)
-      e = cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, keys, skeys, vals, ent, (int)m,
-                                          0, end_bit, st);
-    if (e == cudaSuccess) {
-      note_launch();
-      own_goff_kernel<<<grid_stride_blocks((m + 1 + kOT - 1) / kOT, sms * 8), kOT, 0, st>>>(
-          skeys, m, t->n, goff);
-      e = cudaGetLastError();
-    }
-  } else {
-    if (e == cudaSuccess) {
-      note_launch();
-      own_count_kernel<<<g_edges, kOT, 0, st>>>(eoff, ecols, echunk_rows, koff, t->n, me, cnt,
-                                                t->d_status);
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess)
-      e = cub::DeviceScan::ExclusiveSum(cub_tmp, cub_bytes, cnt, goff, (int)(n + 1), st);
-    if (e == cudaSuccess) {
-      note_launch();
-      own_scatter_kernel<<<g_edges, kOT, 0, st>>>(eoff, ecols, echunk_rows, koff, t->n, me,
-                                                  goff, cnt, ent, t->d_status);
-      e = cudaGetLastError();
-    }
+  if (e == cudaSuccess) {
+    note_launch();
+    own_count_kernel<<<g_edges, kOT, 0, st>>>(eoff, ecols, echunk_rows, koff, t->n, me, cnt,
+                                              t->d_status);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cub::DeviceScan::ExclusiveSum(cub_tmp, cub_bytes, cnt, goff, (int)(n + 1), st);
+  if (e == cudaSuccess) {
+    note_launch();
+    own_scatter_kernel<<<g_edges, kOT, 0, st>>>(eoff, ecols, echunk_rows, koff, t->n, me, goff,
+                                                cnt, ent, t->d_status);
+    e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     note_launch();
