@@ -140,8 +140,6 @@ __global__ void __launch_bounds__(kOT)
   classify_owners(desc, goff, ent, n, b, units, wlist, dlist, dunits, ctr);
 }
 
-// OWN: every owner's hits are also added to owner_hits[owner] (per-graph
-// counts of a batch of disjoint graphs are sums over their vertex ranges).
 // Rounds of 32 key chunks a warp keeps in flight, and whether the next
 // rounds' keys are loaded before the current ones are probed.
 constexpr int kOwnerRounds = 2;
@@ -150,6 +148,8 @@ constexpr bool kOwnerPrefetch = false;
 // search and chunk bookkeeping once per 8 keys: scale 24, b 1, 131 -> 120 ms.
 constexpr int kOwnerChunk = 8;
 
+// OWN: every owner's hits are also added to owner_hits[owner] (per-graph
+// counts of a batch of disjoint graphs are sums over their vertex ranges).
 template <bool HIER, int R, bool OWN = false>
 __global__ void __launch_bounds__(kOT, 2)
     tc_owner_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ goff,
