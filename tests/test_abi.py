@@ -118,6 +118,12 @@ def test_new_entry_points_validate_on_the_host(libreset):
     assert libreset.reset_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 3
     cfg.streams, cfg.max_batch_requests = 4, 0
     assert libreset.reset_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 3
+    libreset.reset_server_config_default(ctypes.byref(cfg))
+    assert cfg.pinned_result_bytes == 256 << 20 and cfg.max_batch_cost == 1 << 22
+    for field in ("pinned_result_bytes", "max_batch_cost", "mem_budget_bytes"):
+        libreset.reset_server_config_default(ctypes.byref(cfg))
+        setattr(cfg, field, -1)
+        assert libreset.reset_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 3, field
     # unknown batch option; NULL table
     assert libreset.reset_batch_create_ex(ctypes.c_void_p(8), ctypes.c_void_p(8), 10, 7, 10,
                                           1 << 5, ctypes.byref(out), None) == 3
