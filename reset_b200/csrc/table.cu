@@ -340,7 +340,6 @@ __global__ void __launch_bounds__(kTileThreads)
   extern __shared__ __align__(128) unsigned char smem[];
   int32_t* S = reinterpret_cast<int32_t*>(smem);
   unsigned char* fill = smem + (size_t)R_max * 4 * b;
-  __shared__ int s_run_end;
   __shared__ int s_span[kTileWarps];
   __shared__ int s_wnext;
 
@@ -348,31 +347,27 @@ __global__ void __launch_bounds__(kTileThreads)
   const int s0 = tile_first[blockIdx.x], s1 = tile_first[blockIdx.x + 1];
   int u = s0;
   while (u < s1) {
-    // Next segment: big sets are skipped (built by big_build_kernel); a run
-    // is the maximal span of consecutive tile-sized sets.
-    if (warp == 0) {
-      int r = u;
-      if (len[u] > LT) {
-        r = -(u + 1);
-      } else {
-        for (;;) {
-          int idx = r + lane;
-          bool stop = idx >= s1 || len[idx] > LT;
-          unsigned msk = __ballot_sync(kFull, stop);
-          if (msk) {
-            r += __ffs(msk) - 1;
-            break;
-          }
-          r += 32;
+    // Next segment: big sets are skipped (built by big_build_kernel or
+    // build_huge); a run is the maximal span of consecutive tile-sized
+    // sets.  Every warp finds it (the same answer, from L1-cached lengths),
+    // so no barrier waits for one warp's scan.
+    int r = u;
+    if (len[u] > LT) {
+      r = -(u + 1);
+    } else {
+      for (;;) {
+        int idx = r + lane;
+        bool stop = idx >= s1 || len[idx] > LT;
+        unsigned msk = __ballot_sync(kFull, stop);
+        if (msk) {
+          r += __ffs(msk) - 1;
+          break;
         }
+        r += 32;
       }
-      if (lane == 0) s_run_end = r;
     }
-    __syncthreads();
-    const int r = s_run_end;
     if (r < 0) {  // a big set
       u = -r;
-      __syncthreads();
       continue;
     }
     const int64_t RA = off64[u];
