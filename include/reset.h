@@ -234,6 +234,12 @@ reset_status reset_batch_create(const reset_table *t, const int32_t *d_elems,
 #define RESET_BATCH_DECISIONS_ONLY 1 /* flags only: each pair stops as soon as its
                                         decision is settled; *d_inter is not
                                         written                                 */
+#define RESET_BATCH_OWNER_GROUPED 2  /* the replay groups the pairs by the
+                                        larger set, stages its table in shared
+                                        memory and streams the smaller sets
+                                        through it (full sizes, *d_inter
+                                        written); d_elems 16-byte aligned.
+                                        Faster for many pairs per large set */
 reset_status reset_batch_create_ex(const reset_table *t, const int32_t *d_elems,
                                    int64_t capacity, int32_t num, int32_t den,
                                    int32_t options, reset_batch **out,

@@ -304,16 +304,20 @@ class Batch:
     (`inter` is not written when decisions_only)."""
 
     def __init__(self, t: Table, elems: torch.Tensor, capacity: int, num: int = 7,
-                 den: int = 10, decisions_only: bool = False, stream=None):
+                 den: int = 10, decisions_only: bool = False, owner_grouped: bool = False,
+                 stream=None):
+        """owner_grouped: the replay groups the pairs by the larger set and
+        stages its table in shared memory (full sizes; faster when many
+        pairs share a large set)."""
         _need(elems, torch.int32, "elems")
         self._table = t          # the batch reads the table's device arrays
         self._elems = elems
         self.capacity = int(capacity)
         self.decisions_only = bool(decisions_only)
         h = C.c_void_p()
+        opts = (1 if decisions_only else 0) | (2 if owner_grouped else 0)
         check(_lib().reset_batch_create_ex(t.handle, _ptr(elems), self.capacity, num, den,
-                                           1 if decisions_only else 0, C.byref(h),
-                                           _stream(stream)))
+                                           opts, C.byref(h), _stream(stream)))
         self._h = h
         pa, pb, fl, it = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
         check(_lib().reset_batch_buffers(h, C.byref(pa), C.byref(pb), C.byref(fl),

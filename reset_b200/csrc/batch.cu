@@ -34,6 +34,7 @@ struct reset_batch {
   cudaGraphNode_t count_node = nullptr;
   cudaMemsetParams count_params{};
   cudaGraphExec_t exec = nullptr;
+  rst::PairOwnerScratch owner{};  // RESET_BATCH_OWNER_GROUPED: grouping scratch
 };
 
 using namespace rst;
@@ -49,6 +50,10 @@ void batch_destroy(reset_batch* b) {
   cudaFree(b->flags);
   cudaFree(b->np_dev);
   cudaFree(b->cursor);
+  if (b->owner.base) {
+    pair_owner_free(&b->owner, nullptr);
+    cudaStreamSynchronize(nullptr);
+  }
   delete b;
 }
 }  // namespace
@@ -65,9 +70,13 @@ reset_status reset_batch_create_ex(const reset_table* t, const int32_t* d_elems,
                                    int64_t capacity, int32_t num, int32_t den,
                                    int32_t options, reset_batch** out,
                                    reset_stream_t stream) {
-  if (options & ~RESET_BATCH_DECISIONS_ONLY) return arg_fail("unknown batch option");
+  if (options & ~(RESET_BATCH_DECISIONS_ONLY | RESET_BATCH_OWNER_GROUPED))
+    return arg_fail("unknown batch option");
   if (!t || !out) return arg_fail("NULL table or output");
   if (!d_elems && t->m > 0) return arg_fail("NULL elements");
+  const bool owner = (options & RESET_BATCH_OWNER_GROUPED) != 0;
+  if (owner && ((reinterpret_cast<uintptr_t>(d_elems) & 15) != 0 || t->m > INT32_MAX - 4))
+    return arg_fail("owner-grouped batches need 16-byte aligned elements, at most 2^31 - 5");
   if (capacity < 1 || capacity > INT32_MAX) return arg_fail("capacity must be in 1..2^31-1");
   if (den <= 0 || num < 0) return arg_fail("threshold num/den");
   *out = nullptr;
@@ -90,15 +99,27 @@ reset_status reset_batch_create_ex(const reset_table* t, const int32_t* d_elems,
   }
   // np_dev's high word stays 0; the count node writes the low word
   e = cudaMemset(b->np_dev, 0, sizeof(int64_t));
+  if (e == cudaSuccess && owner) {  // grouping scratch for `capacity` pairs
+    reset_status ps = pair_owner_alloc(t->n, capacity, &b->owner, nullptr);
+    if (ps == RESET_OK) e = cudaStreamSynchronize(nullptr);
+    if (ps != RESET_OK) {
+      batch_destroy(b);
+      return ps;
+    }
+  }
   // capture the kernel, then put the two memset nodes in front of it
   cudaStream_t cap = nullptr;
   reset_status rs = RESET_OK;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rs = sss_launch_persistent(t, d_elems, b->pa, b->pb, b->np_dev, b->cursor, capacity,
-                               num, den, b->flags, b->inter,
-                               (options & RESET_BATCH_DECISIONS_ONLY) != 0, cap);
+    if (owner)
+      rs = pair_owner_launch(t, t->d_desc, d_elems, t->m, b->pa, b->pb, capacity, b->np_dev,
+                             false, num, den, 0.f, b->flags, b->inter, b->owner, cap);
+    else
+      rs = sss_launch_persistent(t, d_elems, b->pa, b->pb, b->np_dev, b->cursor, capacity,
+                                 num, den, b->flags, b->inter,
+                                 (options & RESET_BATCH_DECISIONS_ONLY) != 0, cap);
     cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
     if (e == cudaSuccess) e = e2;
   }

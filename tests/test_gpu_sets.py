@@ -95,14 +95,19 @@ def test_self_join_pipeline_equals_brute_force(R, oracle_mod, cuda, hier, ulog, 
     batch.close()
 
 
-def test_batch_equals_sss_across_replays(R, oracle_mod, cuda):
+@pytest.mark.parametrize("owner_grouped", [False, True])
+def test_batch_equals_sss_across_replays(R, oracle_mod, cuda, owner_grouped):
+    """Replays of different pair counts (including 0 and 1) equal the plain
+    call and the oracle, for the persistent pair kernel and for the
+    owner-grouped replay (pairs grouped by the larger set, its table staged
+    in shared memory)."""
     torch = cuda
     off, cols = R.gen_rmat(12, 16, 0x5EED3000, oriented=False)
     t = R.Table(off, cols, hierarchical=True)
     n = off.numel() - 1
     g = torch.Generator(device="cuda").manual_seed(5)
     cap = 200_000
-    batch = R.Batch(t, cols, capacity=cap, num=1, den=4)
+    batch = R.Batch(t, cols, capacity=cap, num=1, den=4, owner_grouped=owner_grouped)
     ot = oracle_mod.Table(host(off), host(cols), hier=1)
     for P in [cap, 1, 0, 77_777, 31, 32, 33, 150_000]:
         pa = torch.randint(0, n, (P,), device="cuda", dtype=torch.int32, generator=g)
