@@ -547,11 +547,14 @@ __global__ void huge_home_kernel(const int32_t* __restrict__ keys, int64_t d, in
   }
 }
 
+// Carry functions of the buckets; nxt[h] = the next bucket (circular).
 __global__ void huge_fn_kernel(const int32_t* __restrict__ cnt, int64_t l, int b,
-                               CarryFn* __restrict__ fn) {
+                               CarryFn* __restrict__ fn, int32_t* __restrict__ nxt) {
   for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < l;
-       h += (int64_t)gridDim.x * blockDim.x)
+       h += (int64_t)gridDim.x * blockDim.x) {
     fn[h] = CarryFn{0, (long long)cnt[h] - b};
+    nxt[h] = (int32_t)((h + 1) & (l - 1));
+  }
 }
 
 // start[h] = h where the carry into bucket h is 0, else -1 (fn holds the
@@ -589,22 +592,31 @@ __global__ void huge_place_kernel(const int32_t* __restrict__ keys,
                                   const int32_t* __restrict__ run_off,
                                   const int32_t* __restrict__ n_runs, int64_t l, int b,
                                   int64_t bn, int32_t* __restrict__ fill,
-                                  int32_t* __restrict__ G, int32_t* __restrict__ status) {
+                                  int32_t* __restrict__ nxt, int32_t* __restrict__ G,
+                                  int32_t* __restrict__ status) {
   const int64_t nr = *n_runs;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nr;
        r += (int64_t)gridDim.x * blockDim.x) {
     const int32_t s0 = run_off[r], s1 = s0 + run_len[r];
     for (int32_t j = s0; j < s1; ++j) {
       const int32_t i = sorted_idx[j];
+      // first bucket with room at or after the home bucket: full buckets
+      // point further along (nxt, compressed on the way), so a run of
+      // repeated keys does not rescan its cluster for every key
       int64_t h = home[i];
       int64_t guard = 0;
       while (fill[h] >= b && guard < l) {
-        h = (h + 1) & (l - 1);
+        h = nxt[h];
         ++guard;
       }
       if (guard >= l) {
         atomicOr(status, kErrTableFull);
         continue;
+      }
+      for (int64_t x = home[i]; x != h && fill[x] >= b;) {  // compress
+        const int64_t y = nxt[x];
+        nxt[x] = (int32_t)h;
+        x = y;
       }
       const int k = fill[h]++;
       G[h + (int64_t)k * bn] = keys[i];
@@ -843,10 +855,10 @@ reset_status build_huge(const reset_table* t, const int32_t* d_elems, int64_t rs
   RST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb[5], ni, ni, (int)nblk, st));
   size_t tmp = 0;
   for (size_t x : tb) tmp = std::max(tmp, x);
-  // one scratch block: 8 arrays of d ints, 4 of l ints, l carry functions
+  // one scratch block: 8 arrays of d ints, 5 of l ints, l carry functions
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t sd = al(4 * (size_t)d), sl = al(4 * (size_t)l);
-  const size_t bytes = 8 * sd + 4 * sl + al(sizeof(CarryFn) * (size_t)l) +
+  const size_t bytes = 8 * sd + 5 * sl + al(sizeof(CarryFn) * (size_t)l) +
                        2 * al(4 * (size_t)(nblk + 1)) + al(16) + al(tmp);
   char* base = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&base), bytes, st));
@@ -868,6 +880,7 @@ reset_status build_huge(const reset_table* t, const int32_t* d_elems, int64_t rs
   int32_t* start = reinterpret_cast<int32_t*>(carve(sl));
   int32_t* cstart = reinterpret_cast<int32_t*>(carve(sl));
   int32_t* fill = reinterpret_cast<int32_t*>(carve(sl));
+  int32_t* nxt = reinterpret_cast<int32_t*>(carve(sl));
   CarryFn* fn = reinterpret_cast<CarryFn*>(carve(al(sizeof(CarryFn) * (size_t)l)));
   int32_t* blk = reinterpret_cast<int32_t*>(carve(al(4 * (size_t)(nblk + 1))));
   int32_t* blk_off = reinterpret_cast<int32_t*>(carve(al(4 * (size_t)(nblk + 1))));
@@ -882,7 +895,7 @@ reset_status build_huge(const reset_table* t, const int32_t* d_elems, int64_t rs
     huge_home_kernel<HIER><<<grid_for(d, kThreads), kThreads, 0, st>>>(keys, d, lg, t->lg_max,
                                                                       home, cnt);
     note_launch();
-    huge_fn_kernel<<<grid_for(l, kThreads), kThreads, 0, st>>>(cnt, l, b, fn);
+    huge_fn_kernel<<<grid_for(l, kThreads), kThreads, 0, st>>>(cnt, l, b, fn, nxt);
     size_t x = tmp;
     RST_CUDA(cub::DeviceScan::InclusiveScan(ctmp, x, fn, fn, ComposeCarry(), li, st));
     note_launch();
@@ -901,7 +914,7 @@ reset_status build_huge(const reset_table* t, const int32_t* d_elems, int64_t rs
     RST_CUDA(cub::DeviceScan::ExclusiveSum(ctmp, x, run_len, run_off, di, st));
     note_launch();
     huge_place_kernel<<<grid_for(d, kThreads), kThreads, 0, st>>>(
-        keys, home, idx_s, run_len, run_off, n_runs, l, b, bn, fill, G, t->d_status);
+        keys, home, idx_s, run_len, run_off, n_runs, l, b, bn, fill, nxt, G, t->d_status);
     RST_CUDA(cudaGetLastError());
     if (d_hash_out) {
       note_launch();

@@ -73,8 +73,8 @@ def test_table_layout_huge_sets(R, cuda, oracle_mod, hier, alpha, bucket):
     small sets around them."""
     rng = np.random.default_rng(11)
     big = rng.integers(0, 1 << 24, 70000)
-    big[:3000] = big[0]                                   # one key repeated
-    big[3000:6000] = (1 << 20) - 1 - rng.integers(0, 4, 3000)  # high buckets
+    big[:20000] = big[0]               # one key repeated: a cluster of 20000 keys
+    big[20000:23000] = (1 << 20) - 1 - rng.integers(0, 4, 3000)  # high buckets
     rng.shuffle(big)
     other = rng.integers(0, 1 << 20, 80000)
     rows = [np.sort(rng.choice(1 << 20, 40, replace=False)), big, other,
