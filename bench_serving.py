@@ -538,7 +538,8 @@ def ir_serve_ours(a, rank, world, local):
         _, _, cnt = api.ir(t, toff, docs, qd, qo)
         exact = int(cnt.sum().item())
         del qd, qo, cnt
-        nat = _ir_native(h_toff, h_docs, reqs, [])   # burst: capacity cross-check
+        # burst (capacity cross-check) and Poisson arrivals, C++ client
+        nat = _ir_native(h_toff, h_docs, reqs, [4000, 8000, 12000])
         if nat is not None:
             for v in nat.values():
                 if "total_results" in v:
@@ -546,8 +547,9 @@ def ir_serve_ours(a, rank, world, local):
         line["native_client"] = {"driver": "reset_b200/bin/reset_serve_ir", "runs": nat,
                                  "exact_total_results": exact,
                                  "note": "same queries and index, C++ client (4000 queries "
-                                         "of warm-up, then all at once), table built by the "
-                                         "driver (alpha 0.2, bucket 5)"}
+                                         "of warm-up, then all at once or Poisson; a waiter "
+                                         "thread takes each result as it completes), table "
+                                         "built by the driver (alpha 0.2, bucket 5)"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = _ir_cpu(h_toff, h_docs, reqs, a.cpu_seconds)
     t.free()

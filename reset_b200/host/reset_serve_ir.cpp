@@ -9,6 +9,7 @@
 // once, untimed (buffers and memory pools reach their working size).  Prints
 // the reference's total line, then throughput and latency percentiles.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <random>
@@ -71,7 +72,20 @@ int main(int argc, char** argv) {
           wt[i] = srv.submit(RESET_REQ_IR, ix, q.data() + qoff[i], qoff[i + 1] - qoff[i]);
         for (int i = 0; i < nw; i++) reset::check(srv.wait(wt[i]).status);
       }
+      // a waiter thread takes each result (and releases it) as soon as it
+      // is done, as a serving client would, while this thread submits
       std::vector<uint64_t> tickets(nq);
+      std::atomic<int> submitted{0};
+      int bad = 0;
+      std::thread waiter([&] {
+        for (int i = 0; i < nq; i++) {
+          while (submitted.load(std::memory_order_acquire) <= i) std::this_thread::yield();
+          reset::ServedResult r = srv.wait(tickets[i]);
+          if (r.status != RESET_OK) ++bad;
+          total += r.count;
+          lat.push_back(r.latency_us / 1e3);
+        }
+      });
       std::mt19937_64 rng(12345);
       std::exponential_distribution<double> gap(rate > 0 ? rate : 1.0);
       const int64_t t0 = reset_now_ns();
@@ -85,13 +99,10 @@ int main(int argc, char** argv) {
         }
         tickets[i] = srv.submit(RESET_REQ_IR, ix, q.data() + qoff[i], qoff[i + 1] - qoff[i],
                                 nullptr, 0, 7, 10, arrival);
+        submitted.store(i + 1, std::memory_order_release);
       }
-      for (int i = 0; i < nq; i++) {
-        reset::ServedResult r = srv.wait(tickets[i]);
-        reset::check(r.status);
-        total += r.count;
-        lat.push_back(r.latency_us / 1e3);
-      }
+      waiter.join();
+      if (bad) throw std::runtime_error("served requests failed");
       wall = (reset_now_ns() - t0) / 1e9;
       reset_server_counters c = srv.stats();
       printf("batches: %lld, mean batch: %.1f\n", (long long)c.batches, c.mean_batch);
