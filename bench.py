@@ -89,7 +89,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep --alpha/--bucket and the library's probe knobs")
     ap.add_argument("--workload", default="tc",
-                    choices=["tc", "sss-join", "ir-serve", "mixed-serve", "tc-batch"],
+                    choices=["tc", "sss-join", "ir-serve", "mixed-serve", "tc-batch", "pattern"],
                     help="tc: TC on R-MAT (default); sss-join: batched Jaccard self-join; "
                          "ir-serve: served conjunctive IR; mixed-serve: served mixed "
                          "intersections on R-MAT scale 22")
@@ -109,6 +109,8 @@ def parse():
     ap.add_argument("--max-batch", type=int, default=1024)
     ap.add_argument("--graphs", type=int, default=1024,
                     help="tc-batch: number of disjoint R-MAT graphs (scales 8..12)")
+    ap.add_argument("--pattern-scale", type=int, default=14,
+                    help="pattern: R-MAT scale of the graphs the patterns are counted on")
     ap.add_argument("--max-batch-cost", type=int, default=1 << 22,
                     help="served forms: estimated probes per batch at most (0 = no limit)")
     return ap.parse_args()

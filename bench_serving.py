@@ -1,6 +1,6 @@
 """Workloads of bench.py beyond the default triangle count (imported by
-bench.py for --workload sss-join | ir-serve | mixed-serve; same JSON-line
-contract, same timing rules).
+bench.py for --workload sss-join | ir-serve | mixed-serve | tc-batch |
+pattern; same JSON-line contract, same timing rules).
 
   sss-join    Batched Jaccard self-join (threshold 7/10, exact integer rule)
               over seeded token sets: prefix-filter candidates, then every
@@ -14,6 +14,8 @@ contract, same timing rules).
   mixed-serve A served mix on R-MAT scale 22: per-vertex triangle jobs,
               three-way (4-clique candidate) intersections and raw pairs
               with sizes log-uniform over 2^4..2^20.
+  tc-batch    Many small graphs counted in one batched call.
+  pattern     SMOG's query patterns Q0..Q8 (subgraph matching) on R-MAT.
 Inputs are synthetic (seeded generators with the shapes of the reference's
 datasets, which are not available).
 """
@@ -833,9 +835,82 @@ def tc_batch_ours(a, rank, world, local):
     _finish(line, rank, world)
 
 
+SEED_PAT = 0x5EED7C00
+
+
+def _pattern_checks(api, pattern):
+    """Second encodings of the clique patterns, counted by other kernels:
+    Q0 by the triangle count, Q3 by the 4-clique kernel, Q5 and Q7 listed
+    level by level (no reuse) through the general pattern kernel."""
+    def listed(k):
+        offs = [0, 1] + [1 + sum(range(2, l + 1)) for l in range(2, k)]
+        return api.PatternSpec(k, tuple(offs), tuple([0] + [j for l in range(2, k) for j in range(l)]))
+    return {"Q0": lambda t, o, c: api.tc_count(t, o, c),
+            "Q3": lambda t, o, c: api.clique4_count(t, o, c),
+            "Q5": lambda t, o, c: api.pattern_count(t, o, c, listed(5)),
+            "Q7": lambda t, o, c: api.pattern_count(t, o, c, listed(6))}.get(pattern)
+
+
+def pattern_ours(a, rank, world, local):
+    """SMOG's query patterns Q0..Q8 (reset_pattern_count) on seeded R-MAT
+    graphs of scale a.pattern_scale, each on the graph the reference counts
+    it on (oriented for the cliques, symmetric for the rest).  Per pattern,
+    the median of a.steps calls (CUDA events around the whole call:
+    row-order pass, scratch, kernel, count read back); the clique patterns'
+    counts are checked against second encodings run by other kernels."""
+    torch = _setup(local, world)
+    from reset_b200 import api, _lib
+    L = _lib.load()
+    S = a.pattern_scale
+    graphs = {}
+    for g in ("oriented", "symmetric"):
+        off, cols = api.gen_rmat(S, 16, SEED_PAT + S, oriented=(g == "oriented"))
+        graphs[g] = (off, cols, api.Table(off, cols))
+    rows, total_ms, launches = {}, 0.0, 0
+    with B.Clocks(local) as clk:
+        for name, p in api.PATTERNS.items():
+            off, cols, t = graphs[p.graph]
+            for _ in range(max(a.warmup, 1)):
+                want = api.pattern_count(t, off, cols, name)
+            ms = []
+            l0 = L.reset_kernel_launches()
+            for _ in range(a.steps):
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                got = api.pattern_count(t, off, cols, name)
+                e1.record()
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                assert got == want, name
+            launches += L.reset_kernel_launches() - l0
+            chk = _pattern_checks(api, name)
+            rows[name] = {"graph": p.graph, "count": want, "ms": statistics.median(ms),
+                          "start_edges": int(cols.numel())}
+            if chk is not None:
+                other = chk(t, off, cols)
+                assert other == want, f"{name}: {want} vs {other}"
+                rows[name]["checked_by_second_encoding"] = True
+            total_ms += rows[name]["ms"]
+    [total_ms] = _maxr([total_ms], world)
+    line = {
+        "metric": "SMOG query patterns Q0-Q8: summed time per call",
+        "value": total_ms, "unit": "ms", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": total_ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT graphs generated on device)",
+        "config": {"workload": f"patterns_rmat_s{S}_ef16", "scale": S,
+                   "vertices": 1 << S, "patterns": rows,
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    _finish(line, rank, world)
+
+
 def run_ours(a, rank, world, local):
     {"sss-join": sss_join_ours, "ir-serve": ir_serve_ours,
-     "mixed-serve": mixed_serve_ours, "tc-batch": tc_batch_ours}[a.workload](a, rank, world, local)
+     "mixed-serve": mixed_serve_ours, "tc-batch": tc_batch_ours,
+     "pattern": pattern_ours}[a.workload](a, rank, world, local)
 
 
 def run_reference(a, rank, world):
@@ -875,6 +950,24 @@ def run_reference(a, rank, world):
         reqs = _ir_queries(np.diff(toff).astype(np.int64), 5000, rng)
         cb = _ir_cpu(toff, docs, reqs, a.cpu_seconds)
         unit, metric = "queries/s", "IR queries/sec"
+    elif a.workload == "pattern":
+        # the oracle's count by definition (all host threads) per pattern on
+        # the same seeded graphs, at a smaller scale (bounded CPU time)
+        from reset_b200.api import PATTERNS
+        S = min(a.pattern_scale, 11)
+        per, el = {}, 0.0
+        for name, p in PATTERNS.items():
+            off, cols = oracle.rmat_graph(S, 16, SEED_PAT + S, oriented=(p.graph == "oriented"))
+            t0 = time.perf_counter()
+            c = oracle.pattern_count(off, cols, p.k, p.flags, p.offsets, p.backward,
+                                     p.restriction, p.reuse)
+            per[name] = {"count": c, "s": time.perf_counter() - t0}
+            el += per[name]["s"]
+        cores = os.cpu_count() or 1
+        cb = {"value": el * 1e3, "unit": "ms", "cores": cores, "kind": "port",
+              "sample": f"Q0-Q8 at scale {S} (GPU arm: scale {a.pattern_scale}), oracle by "
+                        f"definition: " + ", ".join(f"{k} {v['s']:.2f} s" for k, v in per.items())}
+        unit, metric = "ms", "SMOG query patterns Q0-Q8: summed time per call"
     elif a.workload == "tc-batch":
         t0 = time.perf_counter()
         edges, gi = 0, 0
@@ -902,7 +995,8 @@ def run_reference(a, rank, world):
               "sample": f"{done} raw-pair requests through the oracle in {el:.1f} s"}
         unit, metric = "requests/s", "mixed intersection requests/sec"
     line = {"metric": metric, "value": cb["value"], "unit": unit, "n_gpus": world,
-            "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "steps": 1, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": a.workload != "pattern",
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (CPU generators)", "impl": "reference",
             "config": {"workload": a.workload, "parallelism": "cpu",

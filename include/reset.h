@@ -304,6 +304,57 @@ reset_status reset_clique_count(const reset_table *t, const int32_t *d_off,
                                 const int32_t *d_cols, int64_t m, int32_t k,
                                 uint64_t *d_count, reset_stream_t stream);
 
+/* A query pattern for reset_pattern_count, in the encoding of SMOG's
+ * pattern table (SMOG/SMOG_hie/script_hie.py:85-152, which writes it to
+ * constants.cpp as intersection_orders, intersection_offset, restriction
+ * and reuse, with H and the withRestriction / withDuplicate defines):
+ *   k            pattern vertices (H), 3..RESET_PATTERN_MAX; vertices 0 and
+ *                1 are the two ends of the start edge;
+ *   offsets      k entries: backward[offsets[l-1] .. offsets[l]) are the
+ *                earlier pattern vertices adjacent to vertex l (l >= 1;
+ *                level 1 must be [0]); -1 stands for the vertices that
+ *                the reused level's set already covers;
+ *   backward     offsets[k-1] entries;
+ *   restriction  k entries or NULL (all -1): r = restriction[l] >= 0
+ *                requires m_l < m_r when flags has RESET_PATTERN_RESTRICT;
+ *                with RESET_PATTERN_DISTINCT a level whose r is -1
+ *                requires m_l to differ from m_0 .. m_{l-1}
+ *                (checkRestriction, subgraph_match_hie.cu:23-42);
+ *   reuse        k entries or NULL (all -1): reuse[l] = r in [2, l) makes
+ *                level l start from level r's candidate set; such a level
+ *                lists exactly one -1, every other level none. */
+#define RESET_PATTERN_RESTRICT 1
+#define RESET_PATTERN_DISTINCT 2
+#define RESET_PATTERN_MAX 8
+typedef struct reset_pattern {
+  int32_t k;
+  int32_t flags;
+  const int32_t *offsets;
+  const int32_t *backward;
+  const int32_t *restriction;
+  const int32_t *reuse;
+} reset_pattern;
+
+/* Embeddings of pattern `p` in the graph whose table is `t` (built on
+ * d_off/d_cols): the number of tuples (m_0 .. m_{k-1}) with (m_0, m_1) a
+ * stored edge and, for l >= 2, m_l in
+ *   C_l = [C_reuse(l) or all vertices] ∩ (∩ over listed j of N(m_j)),
+ * each level passing its restriction / distinctness check.  SMOG's
+ * DFSKernelForGeneral and DFSKernelForClique
+ * (SMOG/SMOG_hie/subgraph_match_hie.cu:58-406) as one warp-level DFS per
+ * start edge; C_l starts from the smallest listed row (or the reused set)
+ * and probes the other listed rows' tables.  Symmetric CSR for general
+ * patterns, oriented for cliques, as the reference loads them
+ * (SMOG/SMOG_hie/common_hie.cu:61-85).  Rows in any order; strictly
+ * ascending rows take shortcuts (restriction prefixes, counts without a
+ * scan).  A reusing k-clique chain without checks runs
+ * reset_clique_count.  *d_count (device u64) is overwritten.  Synchronises
+ * `stream` once (scratch sizing and the row-order check). */
+reset_status reset_pattern_count(const reset_table *t, const int32_t *d_off,
+                                 const int32_t *d_cols, int64_t m,
+                                 const reset_pattern *p, uint64_t *d_count,
+                                 reset_stream_t stream);
+
 /* |A ∩ B| counted with A's multiplicity for one pair of device arrays
  * (keys >= 0).  Builds B's table with `params` and probes A.  *d_count
  * (device i64) is overwritten.  Replaces make_hashtable_kernel +

@@ -88,6 +88,9 @@ def lib():
         L.ro_clique4.restype = C.c_uint64
         L.ro_clique_k.argtypes = [C.c_int32, _i32p, _i32p, C.c_int32]
         L.ro_clique_k.restype = C.c_uint64
+        L.ro_pattern_count.argtypes = [C.c_int32, _i32p, _i32p, C.c_int32, C.c_int32,
+                                       _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32]
+        L.ro_pattern_count.restype = C.c_uint64
         L.ro_relabel.argtypes = [C.c_uint64, C.c_int32, C.c_uint32]
         L.ro_relabel.restype = C.c_uint32
         L.ro_mix64.argtypes = [C.c_uint64]
@@ -229,6 +232,20 @@ def clique_k(off, cols, k: int) -> int:
     cols = _c(cols, np.int32)
     return int(lib().ro_clique_k(off.size - 1, off, cols if cols.size else np.zeros(1, np.int32),
                                  k))
+
+
+def pattern_count(off, cols, k, flags, offsets, backward, restriction=None, reuse=None,
+                  nthreads=0) -> int:
+    """Embeddings of a pattern in SMOG's encoding (ro_pattern_count); rows
+    must be sorted."""
+    off = _c(off, np.int32)
+    cols = _c(cols, np.int32)
+    offsets = _c(offsets, np.int32)
+    backward = _c(backward, np.int32)
+    keep = [_c(a, np.int32) if a is not None else None for a in (restriction, reuse)]
+    ptrs = [a.ctypes.data_as(C.c_void_p) if a is not None else None for a in keep]
+    return int(lib().ro_pattern_count(off.size - 1, off, cols if cols.size else np.zeros(1, np.int32),
+                                      k, flags, offsets, backward, ptrs[0], ptrs[1], nthreads))
 
 
 def jaccard_join(off, tok, num=7, den=10):

@@ -497,6 +497,113 @@ uint64_t ro_clique_k(int32_t n, const int32_t *off, const int32_t *cols, int32_t
   return total;
 }
 
+/* Pattern embeddings by definition, for the subgraph matching of SMOG
+ * (SMOG/SMOG_hie/subgraph_match_hie.cu:58-406, the pattern encoding of
+ * SMOG/SMOG_hie/script_hie.py:85-152): m_0 m_1 run over the stored edges;
+ * for l >= 2 the candidates C_l are the keys of the reused level's set
+ * (reuse[l] >= 0) or of the FIRST listed vertex's row, kept when every
+ * listed vertex's row holds them (binary search); each m_l must pass the
+ * level's check, checkRestriction (subgraph_match_hie.cu:23-42).  C_l is
+ * stored whole (unfiltered), as a reused set is. */
+typedef struct {
+  const int32_t *off, *cols, *offsets, *backward, *restriction, *reuse;
+  int32_t n, k, flags, maxd;
+} ro_pat;
+
+static int ro_row_has(const int32_t *off, const int32_t *cols, int32_t y, int32_t x) {
+  int32_t lo = off[y], hi = off[y + 1];
+  while (lo < hi) {
+    const int32_t mid = lo + (hi - lo) / 2;
+    if (cols[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < off[y + 1] && cols[lo] == x;
+}
+
+static int ro_pat_ok(const ro_pat *p, int32_t l, int32_t x, const int32_t *map) {
+  const int32_t r = p->restriction ? p->restriction[l] : -1;
+  if ((p->flags & 2) && r < 0)
+    for (int32_t i = 0; i < l; i++)
+      if (map[i] == x) return 0;
+  if ((p->flags & 1) && r >= 0 && x >= map[r]) return 0;
+  return 1;
+}
+
+static uint64_t ro_pat_level(const ro_pat *p, int32_t l, int32_t *map, int32_t *buf,
+                             int32_t *cnt) {
+  const int32_t a = p->offsets[l - 1], z = p->offsets[l];
+  const int32_t r = p->reuse ? p->reuse[l] : -1;
+  const int32_t *base;
+  int32_t nbase;
+  if (r >= 0) {
+    base = buf + (size_t)r * p->maxd;
+    nbase = cnt[r];
+  } else {
+    int32_t first = -1;
+    for (int32_t i = a; i < z && first < 0; i++)
+      if (p->backward[i] >= 0) first = map[p->backward[i]];
+    base = p->cols + p->off[first];
+    nbase = p->off[first + 1] - p->off[first];
+  }
+  int32_t *C = buf + (size_t)l * p->maxd;
+  int32_t nc = 0;
+  for (int32_t t = 0; t < nbase; t++) {
+    const int32_t x = base[t];
+    int keep = 1;
+    for (int32_t i = a; i < z && keep; i++)
+      if (p->backward[i] >= 0) keep = ro_row_has(p->off, p->cols, map[p->backward[i]], x);
+    if (keep) C[nc++] = x;
+  }
+  cnt[l] = nc;
+  uint64_t total = 0;
+  for (int32_t t = 0; t < nc; t++) {
+    if (!ro_pat_ok(p, l, C[t], map)) continue;
+    if (l == p->k - 1) {
+      total++;
+    } else {
+      map[l] = C[t];
+      total += ro_pat_level(p, l + 1, map, buf, cnt);
+    }
+  }
+  return total;
+}
+
+static void ro_pat_body(void *ctx, int64_t lo, int64_t hi, uint64_t *acc) {
+  const ro_pat *p = (const ro_pat *)ctx;
+  int32_t *buf = (int32_t *)malloc(sizeof(int32_t) * (size_t)p->maxd * (size_t)p->k);
+  int32_t map[64], cnt[64];
+  for (int64_t u = lo; u < hi; u++) {
+    for (int32_t e = p->off[u]; e < p->off[u + 1]; e++) {
+      map[0] = (int32_t)u;
+      map[1] = p->cols[e];
+      if (!ro_pat_ok(p, 1, map[1], map)) continue;
+      *acc += ro_pat_level(p, 2, map, buf, cnt);
+    }
+  }
+  free(buf);
+}
+
+uint64_t ro_pattern_count(int32_t n, const int32_t *off, const int32_t *cols,
+                          int32_t k, int32_t flags, const int32_t *offsets,
+                          const int32_t *backward, const int32_t *restriction,
+                          const int32_t *reuse, int32_t nthreads) {
+  if (k < 3 || k > 64 || n <= 0) return 0;
+  ro_pat p;
+  p.off = off;
+  p.cols = cols;
+  p.offsets = offsets;
+  p.backward = backward;
+  p.restriction = restriction;
+  p.reuse = reuse;
+  p.n = n;
+  p.k = k;
+  p.flags = flags;
+  p.maxd = 1;
+  for (int32_t u = 0; u < n; u++)
+    if (off[u + 1] - off[u] > p.maxd) p.maxd = off[u + 1] - off[u];
+  return ro_parallel(n, 16, ro_pat_body, &p, nthreads);
+}
+
 /* ------------------------------------------------------------------------ */
 /* synthetic inputs                                                          */
 /* ------------------------------------------------------------------------ */

@@ -117,6 +117,15 @@ uint64_t ro_clique4(int32_t n, const int32_t *off, const int32_t *cols);
 /* k-cliques (k >= 3) of an oriented graph with sorted rows, each counted
  * once (SMOG/SMOG_hie/subgraph_match_hie.cu:58-247). */
 uint64_t ro_clique_k(int32_t n, const int32_t *off, const int32_t *cols, int32_t k);
+/* Embeddings of a pattern in SMOG's encoding (k vertices; backward lists
+ * by offsets; restriction / reuse arrays or NULL; flags 1 = restrictions,
+ * 2 = distinctness) in a graph with sorted rows, counted by the definition
+ * (SMOG/SMOG_hie/subgraph_match_hie.cu:23-42, 58-406); nthreads <= 0 = all
+ * cores. */
+uint64_t ro_pattern_count(int32_t n, const int32_t *off, const int32_t *cols,
+                          int32_t k, int32_t flags, const int32_t *offsets,
+                          const int32_t *backward, const int32_t *restriction,
+                          const int32_t *reuse, int32_t nthreads);
 
 /* ---- synthetic inputs --------------------------------------------------- */
 

@@ -44,6 +44,12 @@ class TableView(C.Structure):
                 ("d_off", C.c_void_p)]
 
 
+class Pattern(C.Structure):
+    _fields_ = [("k", C.c_int32), ("flags", C.c_int32),
+                ("offsets", C.POINTER(C.c_int32)), ("backward", C.POINTER(C.c_int32)),
+                ("restriction", C.POINTER(C.c_int32)), ("reuse", C.POINTER(C.c_int32))]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("streams", C.c_int32), ("max_batch_requests", C.c_int32),
                 ("mem_budget_bytes", C.c_int64), ("max_batch_cost", C.c_int64),
@@ -100,6 +106,7 @@ SIGNATURES = {
     "reset_tc_count_batch": (I32, [P, P, P, I64, P, I32, P, P]),
     "reset_clique4_count": (I32, [P, P, P, I64, P, P]),
     "reset_clique_count": (I32, [P, P, P, I64, I32, P, P]),
+    "reset_pattern_count": (I32, [P, P, P, I64, C.POINTER(Pattern), P, P]),
     "reset_sss": (I32, [P, P, P, P, P, I64, I32, I32, P, P, P]),
     "reset_sss_float": (I32, [P, P, P, P, P, I64, C.c_float, P, P, P]),
     "reset_ir": (I32, [P, P, P, P, P, I32, P, P, P, P]),

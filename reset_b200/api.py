@@ -8,11 +8,11 @@ given.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional, Tuple
+from typing import NamedTuple, Optional, Tuple
 
 import torch
 
-from ._lib import Params, TableView, Tuning, check, load
+from ._lib import Params, Pattern, TableView, Tuning, check, load
 
 
 def _lib():
@@ -188,6 +188,75 @@ def clique_count(t: Table, off: torch.Tensor, cols: torch.Tensor, k: int, stream
     out = torch.zeros(1, dtype=torch.int64, device=cols.device)
     check(_lib().reset_clique_count(t.handle, _ptr(off), _ptr(cols), cols.numel(), k,
                                     _ptr(out), _stream(stream)))
+    return int(out.item()) & ((1 << 64) - 1)
+
+
+PATTERN_RESTRICT = 1  # withRestriction: m_l < m_restriction[l]
+PATTERN_DISTINCT = 2  # withDuplicate: levels without a restriction take new vertices
+
+
+class PatternSpec(NamedTuple):
+    """A query pattern in SMOG's encoding (reset_pattern in reset.h):
+    backward[offsets[l-1]:offsets[l]] are the earlier vertices adjacent to
+    vertex l, -1 standing for those a reused level's set covers."""
+    k: int
+    offsets: Tuple[int, ...]
+    backward: Tuple[int, ...]
+    restriction: Optional[Tuple[int, ...]] = None
+    reuse: Optional[Tuple[int, ...]] = None
+    flags: int = 0
+    graph: str = "symmetric"  # the CSR the pattern is counted on
+
+
+_RD = PATTERN_RESTRICT | PATTERN_DISTINCT
+# SMOG's query patterns (SMOG/SMOG_hie/script_hie.py:85-152), each with the
+# graph the reference counts it on (SMOG/SMOG_hie/common_hie.cu:72-85: the
+# oriented files for Q0, Q3, Q5 and Q7 -- triangles and 4-, 5-, 6-cliques --
+# the symmetric ones for the rest).
+PATTERNS = {
+    "Q0": PatternSpec(3, (0, 1, 3), (0, 0, 1), graph="oriented"),
+    "Q1": PatternSpec(4, (0, 1, 2, 4), (0, 0, 1, 2), (-1, 0, 1, 0), None, PATTERN_RESTRICT),
+    "Q2": PatternSpec(4, (0, 1, 3, 5), (0, 0, 1, 1, 2), (-1, -1, 1, 0), None, PATTERN_RESTRICT),
+    "Q3": PatternSpec(4, (0, 1, 3, 5), (0, 0, 1, -1, 2), None, (-1, -1, -1, 2),
+                      graph="oriented"),
+    "Q4": PatternSpec(5, (0, 1, 3, 5, 6), (0, 0, 1, -1, 2, -1), (-1, 0, -1, 2, -1),
+                      (-1, -1, -1, 2, 2), _RD),
+    "Q5": PatternSpec(5, (0, 1, 3, 5, 7), (0, 0, 1, -1, 2, -1, 3), None, (-1, -1, -1, 2, 3),
+                      graph="oriented"),
+    "Q6": PatternSpec(5, (0, 1, 3, 4, 6), (0, 0, 1, -1, 2, 3), (-1, 0, -1, 2, -1),
+                      (-1, -1, -1, 2, -1), _RD),
+    "Q7": PatternSpec(6, (0, 1, 3, 5, 7, 9), (0, 0, 1, -1, 2, -1, 3, -1, 4), None,
+                      (-1, -1, -1, 2, 3, 4), graph="oriented"),
+    "Q8": PatternSpec(5, (0, 1, 3, 5, 6), (0, 0, 1, -1, 2, -1), (-1, 0, -1, -1, 3),
+                      (-1, -1, -1, 2, 3), PATTERN_RESTRICT),
+}
+
+
+def pattern_struct(p: PatternSpec):
+    """-> (reset_pattern, the int32 arrays it points to); checks the array
+    lengths the C side cannot."""
+    k = p.k
+    if len(p.offsets) != k:
+        raise ValueError("offsets needs k entries")
+    if len(p.backward) < p.offsets[-1]:
+        raise ValueError("backward needs offsets[k-1] entries")
+    for a in (p.restriction, p.reuse):
+        if a is not None and len(a) != k:
+            raise ValueError("restriction and reuse need k entries")
+    arrs = [None if a is None else (C.c_int32 * max(len(a), 1))(*a)
+            for a in (p.offsets, p.backward, p.restriction, p.reuse)]
+    ptrs = [C.cast(a, C.POINTER(C.c_int32)) if a is not None else None for a in arrs]
+    return Pattern(k, p.flags, *ptrs), arrs
+
+
+def pattern_count(t: Table, off: torch.Tensor, cols: torch.Tensor, pattern, stream=None) -> int:
+    """Embeddings of `pattern` (a PatternSpec or a PATTERNS name) in the
+    graph the table was built on (SMOG's subgraph matching)."""
+    p = PATTERNS[pattern] if isinstance(pattern, str) else pattern
+    ps, _keep = pattern_struct(p)
+    out = torch.zeros(1, dtype=torch.int64, device=cols.device)
+    check(_lib().reset_pattern_count(t.handle, _ptr(off), _ptr(cols), cols.numel(), C.byref(ps),
+                                     _ptr(out), _stream(stream)))
     return int(out.item()) & ((1 << 64) - 1)
 
 

@@ -255,6 +255,26 @@ __global__ void max_degree_kernel(const int32_t* __restrict__ off, int32_t n,
   if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
 }
 
+// Largest row length of a CSR (d_off, n rows) into *out; synchronises `st`.
+reset_status max_row_length(const int32_t* d_off, int32_t n, cudaStream_t st, int32_t* out) {
+  *out = 0;
+  int32_t* d_mx = nullptr;
+  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_mx), sizeof(int32_t), st));
+  cudaError_t e = cudaMemsetAsync(d_mx, 0, sizeof(int32_t), st);
+  if (e == cudaSuccess) {
+    note_launch();
+    max_degree_kernel<<<sm_count() * 4, 256, 0, st>>>(d_off, n, d_mx);
+    e = cudaGetLastError();
+  }
+  int32_t mx = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&mx, d_mx, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFreeAsync(d_mx, st);
+  if (e != cudaSuccess) return cuda_fail(e, "max degree", __FILE__, __LINE__);
+  *out = mx;
+  return RESET_OK;
+}
+
 }  // namespace
 }  // namespace rst
 
@@ -271,19 +291,11 @@ extern "C" reset_status reset_clique4_count(const reset_table* t, const int32_t*
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
-  int32_t* d_mx = nullptr;
-  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_mx), sizeof(int32_t), st));
-  cudaError_t e = cudaMemsetAsync(d_mx, 0, sizeof(int32_t), st);
-  if (e == cudaSuccess) {
-    note_launch();
-    max_degree_kernel<<<sm_count() * 4, 256, 0, st>>>(d_off, t->n, d_mx);
-    e = cudaGetLastError();
-  }
   int32_t mx = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&mx, d_mx, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(d_mx, st);
-  if (e != cudaSuccess) return cuda_fail(e, "max degree", __FILE__, __LINE__);
+  {
+    const reset_status s = max_row_length(d_off, t->n, st, &mx);
+    if (s != RESET_OK) return s;
+  }
   const int32_t cap = mx > 0 ? mx : 1;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -295,7 +307,7 @@ extern "C" reset_status reset_clique4_count(const reset_table* t, const int32_t*
   int32_t* d_scr = nullptr;
   unsigned long long* d_cur = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_scr), sizeof(int32_t) * warps * cap, st));
-  e = scratch_malloc(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
+  cudaError_t e = scratch_malloc(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_cur, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) {
     note_launch();
@@ -327,19 +339,11 @@ extern "C" reset_status reset_clique_count(const reset_table* t, const int32_t* 
   cudaStream_t st = as_stream(stream);
   RST_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st));
   if (m == 0 || t->n == 0) return RESET_OK;
-  int32_t* d_mx = nullptr;
-  RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_mx), sizeof(int32_t), st));
-  cudaError_t e = cudaMemsetAsync(d_mx, 0, sizeof(int32_t), st);
-  if (e == cudaSuccess) {
-    note_launch();
-    max_degree_kernel<<<sm_count() * 4, 256, 0, st>>>(d_off, t->n, d_mx);
-    e = cudaGetLastError();
-  }
   int32_t mx = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&mx, d_mx, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(d_mx, st);
-  if (e != cudaSuccess) return cuda_fail(e, "max degree", __FILE__, __LINE__);
+  {
+    const reset_status s = max_row_length(d_off, t->n, st, &mx);
+    if (s != RESET_OK) return s;
+  }
   const int32_t cap = mx > 0 ? mx : 1;
   const void* kf = t->hier ? (const void*)clique_k_kernel<true> : (const void*)clique_k_kernel<false>;
   int per_sm = 0;
@@ -352,7 +356,7 @@ extern "C" reset_status reset_clique_count(const reset_table* t, const int32_t* 
   unsigned long long* d_cur = nullptr;
   RST_CUDA(scratch_malloc(reinterpret_cast<void**>(&d_scr),
                           sizeof(int32_t) * (size_t)warps * (size_t)cap * (size_t)levels, st));
-  e = scratch_malloc(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
+  cudaError_t e = scratch_malloc(reinterpret_cast<void**>(&d_cur), sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_cur, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) {
     note_launch();

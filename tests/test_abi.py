@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import pytest
 from conftest import ROOT
 
 
@@ -82,7 +83,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     structs = {"reset_params": _lib.Params, "reset_tuning": _lib.Tuning,
                "reset_table_view": _lib.TableView, "reset_server_config": _lib.ServerConfig,
                "reset_request": _lib.Request, "reset_result": _lib.Result,
-               "reset_server_counters": _lib.ServerCounters}
+               "reset_server_counters": _lib.ServerCounters, "reset_pattern": _lib.Pattern}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "reset.h"',
              'int main(void) {']
     for cname, py in structs.items():
@@ -141,3 +142,39 @@ def test_new_entry_points_validate_on_the_host(libreset):
     libreset.reset_get_tuning(ctypes.byref(t))
     bad = _lib.Tuning(t.probe_rounds, t.warp_pair_min, 7)
     assert libreset.reset_set_tuning(ctypes.byref(bad)) == 3
+
+
+def test_pattern_count_validates_on_the_host(libreset):
+    """reset_pattern_count rejects malformed patterns before any CUDA call
+    (a NULL table is checked first, so a dummy handle stands in)."""
+    from reset_b200 import api
+    fake = ctypes.c_void_p(8)
+    cnt = ctypes.c_void_p(8)
+
+    def status(spec):
+        ps, _keep = api.pattern_struct(spec)
+        return libreset.reset_pattern_count(fake, None, None, 0, ctypes.byref(ps), cnt, None)
+
+    P = api.PatternSpec
+    bad = [
+        P(2, (0, 1), (0,)),                                  # k < 3
+        P(9, tuple(range(9)), (0,) * 8),                     # k > RESET_PATTERN_MAX
+        P(3, (0, 1, 3), (1, 0, 1)),                          # level 1 must be [0]
+        P(3, (0, 1, 3), (0, 0, 2)),                          # backward not earlier
+        P(3, (0, 1, 3), (0, 0, -1)),                         # -1 without reuse
+        P(4, (0, 1, 3, 4), (0, 0, 1, 2), None, (-1, -1, -1, 2)),  # reuse without -1
+        P(4, (0, 1, 3, 5), (0, 0, 1, -1, 2), None, (-1, -1, -1, 3)),  # reuse not earlier
+        P(4, (0, 1, 3, 3), (0, 0, 1)),                       # empty level, no reuse
+        P(3, (0, 1, 3), (0, 0, 1), (0, -1, -1), None, 1),    # restriction[0]
+        P(3, (0, 1, 3), (0, 0, 1), (-1, 0, 2), None, 1),     # restriction not earlier
+        P(3, (0, 1, 3), (0, 0, 1), None, None, 4),           # unknown flag
+    ]
+    for spec in bad:
+        assert status(spec) == 3, spec
+    assert libreset.reset_pattern_count(fake, None, None, 0, None, cnt, None) == 3
+    ps, _keep = api.pattern_struct(api.PATTERNS["Q4"])
+    assert libreset.reset_pattern_count(None, None, None, 0, ctypes.byref(ps), cnt, None) == 3
+    with pytest.raises(ValueError):
+        api.pattern_struct(P(4, (0, 1, 3), (0, 0, 1)))
+    with pytest.raises(ValueError):
+        api.pattern_struct(P(3, (0, 1, 3), (0, 0, 1), (-1, 0)))

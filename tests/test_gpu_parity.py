@@ -545,6 +545,116 @@ def test_clique_k_complete_graph_and_limits(R, cuda):
             R.clique_count(t, d_off, d_cols, k)
 
 
+# ------------------------------------------------------------- patterns --
+
+def _extra_patterns(R):
+    """Hand-made patterns beside SMOG's: reuse with restriction and
+    distinctness mixed; last levels that list one vertex (the vertex just
+    picked, bounded by it, or distinct from all earlier ones)."""
+    P = R.PatternSpec
+    return {
+        "mixed": P(5, (0, 1, 2, 4, 6), (0, 0, 1, -1, 3, 0), (-1, 0, -1, 1, -1),
+                   (-1, -1, -1, 2, -1), 3),
+        "tail_bound": P(4, (0, 1, 3, 4), (0, 0, 1, 2), (-1, 0, -1, 2), None, 3),
+        "tail_distinct": P(4, (0, 1, 3, 4), (0, 0, 1, 2), (-1, 0, -1, -1), None, 3),
+        "tail_fixed": P(4, (0, 1, 3, 4), (0, 0, 1, 0), (-1, 0, 1, 1), None, 1),
+    }
+
+
+def _oracle_pattern(oracle_mod, off, cols, p):
+    return oracle_mod.pattern_count(off, cols, p.k, p.flags, p.offsets, p.backward,
+                                    p.restriction, p.reuse)
+
+
+@pytest.mark.parametrize("scale,hier", [(9, True), (10, False), (11, True)])
+def test_pattern_count_matches_oracle(R, cuda, oracle_mod, scale, hier):
+    """SMOG's query patterns (the general and the reusing form, with
+    restrictions and distinctness) equal the oracle's count by definition,
+    each on the graph the reference counts it on (oriented for the cliques
+    Q0, Q3, Q5, Q7; symmetric for the rest).  Q6 stops at scale 10, where
+    the oracle still takes seconds."""
+    torch = cuda
+    graphs = {}
+    for name, p in R.PATTERNS.items():
+        if name == "Q6" and scale > 10:
+            continue
+        if p.graph not in graphs:
+            off, cols = oracle_mod.rmat_graph(scale, 16, 0x5EED7B00 + scale,
+                                              oriented=(p.graph == "oriented"))
+            d_off, d_cols = dev(off, torch), dev(cols, torch)
+            graphs[p.graph] = (off, cols, d_off, d_cols, R.Table(d_off, d_cols, hierarchical=hier))
+        off, cols, d_off, d_cols, t = graphs[p.graph]
+        assert R.pattern_count(t, d_off, d_cols, name) == _oracle_pattern(oracle_mod, off, cols, p), name
+    off, cols, d_off, d_cols, t = graphs["symmetric"]
+    for name, p in _extra_patterns(R).items():
+        assert R.pattern_count(t, d_off, d_cols, p) == _oracle_pattern(oracle_mod, off, cols, p), name
+    for g in graphs.values():
+        g[4].check()
+
+
+def test_pattern_count_complete_graphs_and_cliques(R, cuda, oracle_mod):
+    """Complete graphs (every candidate set full, distinctness and
+    restrictions decide alone), a hand-made pattern mixing reuse,
+    restriction and distinctness, an 8-vertex reusing clique chain equal to
+    the 8-clique count, and Q5 equal to the 5-clique kernel's count."""
+    torch = cuda
+    from math import comb
+    P = R.PatternSpec
+    chain8 = P(8, (0, 1, 3, 5, 7, 9, 11, 13), (0, 0, 1, -1, 2, -1, 3, -1, 4, -1, 5, -1, 6),
+               None, (-1, -1, -1, 2, 3, 4, 5, 6))
+    n = 12
+    for oriented in (True, False):
+        rows = [[v for v in range(n) if (v > u if oriented else v != u)] for u in range(n)]
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum([len(r) for r in rows])
+        cols = np.array(sum(rows, []), np.int32)
+        d_off, d_cols = dev(off, torch), dev(cols, torch)
+        t = R.Table(d_off, d_cols)
+        for name, p in (list(R.PATTERNS.items()) + list(_extra_patterns(R).items()) +
+                        [("chain8", chain8)]):
+            want = _oracle_pattern(oracle_mod, off, cols, p)
+            assert R.pattern_count(t, d_off, d_cols, p) == want, (name, oriented)
+        if oriented:
+            assert R.pattern_count(t, d_off, d_cols, chain8) == comb(n, 8)
+    off, cols = oracle_mod.rmat_graph(12, 16, 0x5EED7B0C, oriented=True)
+    d_off, d_cols = dev(off, torch), dev(cols, torch)
+    t = R.Table(d_off, d_cols)
+    assert R.pattern_count(t, d_off, d_cols, "Q5") == R.clique_count(t, d_off, d_cols, 5)
+    assert R.pattern_count(t, d_off, d_cols, chain8) == R.clique_count(t, d_off, d_cols, 8)
+    # the same cliques listed level by level (no reuse) run the general
+    # kernel, the reusing chains the k-clique kernel
+    for name, k in (("Q3", 4), ("Q5", 5), ("Q7", 6)):
+        offs = [0, 1] + [1 + sum(range(2, l + 1)) for l in range(2, k)]
+        listed = P(k, tuple(offs), tuple([0] + [j for l in range(2, k) for j in range(l)]))
+        assert R.pattern_count(t, d_off, d_cols, listed) == R.pattern_count(t, d_off, d_cols, name), name
+    # an empty edge list counts nothing
+    e_off = dev(np.zeros(5, np.int32), torch)
+    e_cols = torch.empty(0, dtype=torch.int32, device="cuda")
+    assert R.pattern_count(R.Table(e_off, e_cols), e_off, e_cols, "Q4") == 0
+
+
+def test_pattern_count_unsorted_rows(R, cuda, oracle_mod):
+    """Rows in shuffled order (no ascending-row shortcuts: every key
+    scanned) count what the sorted rows count, for every pattern."""
+    torch = cuda
+    rng = np.random.default_rng(0x5EED7B0A)
+    for g in ("symmetric", "oriented"):
+        off, cols = oracle_mod.rmat_graph(10, 16, 0x5EED7B0A, oriented=(g == "oriented"))
+        sh = cols.copy()
+        for u in range(off.size - 1):
+            rng.shuffle(sh[off[u]:off[u + 1]])
+        d_off, d_cols = dev(off, torch), dev(sh, torch)
+        t = R.Table(d_off, d_cols, hierarchical=(g == "symmetric"))
+        for name, p in R.PATTERNS.items():
+            if p.graph == g:
+                assert R.pattern_count(t, d_off, d_cols, name) == \
+                    _oracle_pattern(oracle_mod, off, cols, p), name
+        if g == "symmetric":
+            for name, p in _extra_patterns(R).items():
+                assert R.pattern_count(t, d_off, d_cols, p) == \
+                    _oracle_pattern(oracle_mod, off, cols, p), name
+
+
 def block_diagonal(graphs):
     """Disjoint oriented graphs [(off, cols)] -> one CSR + vertex offsets."""
     offs, colss, gro = [np.zeros(1, np.int64)], [], [0]

@@ -283,6 +283,68 @@ def test_clique4_oracle_small_cases(oracle_mod):
     assert oracle_mod.clique4(off, cols) == want
 
 
+def _pattern_brute_force(off, cols, p):
+    """Embeddings of a pattern by its definition, every vertex tried at
+    every level (tiny graphs only)."""
+    n = off.size - 1
+    adj = [set(cols[off[u]:off[u + 1]].tolist()) for u in range(n)]
+    k = p.k
+    restr = p.restriction or (-1,) * k
+    reuse = p.reuse or (-1,) * k
+
+    def in_c(l, m, x):
+        if reuse[l] >= 0 and not in_c(reuse[l], m, x):
+            return False
+        return all(x in adj[m[j]] for j in p.backward[p.offsets[l - 1]:p.offsets[l]] if j >= 0)
+
+    def ok(l, m, x):
+        r = restr[l]
+        if (p.flags & 2) and r < 0 and x in m[:l]:
+            return False
+        return not ((p.flags & 1) and r >= 0 and x >= m[r])
+
+    def rec(m):
+        if len(m) == k:
+            return 1
+        l = len(m)
+        return sum(rec(m + [x]) for x in range(n) if in_c(l, m, x) and ok(l, m, x))
+
+    return sum(rec([u, v]) for u in range(n) for v in cols[off[u]:off[u + 1]].tolist()
+               if ok(1, [u], v))
+
+
+def test_pattern_oracle_matches_brute_force(oracle_mod):
+    """ro_pattern_count equals the definition for every SMOG query pattern
+    (SMOG/SMOG_hie/script_hie.py:85-152), on the graph the reference counts
+    it on, and for a hand-made pattern mixing reuse, restriction and
+    distinctness."""
+    from reset_b200.api import PATTERNS, PatternSpec
+    P = PatternSpec
+    extra = {"mixed": P(5, (0, 1, 2, 4, 6), (0, 0, 1, -1, 3, 0), (-1, 0, -1, 1, -1),
+                        (-1, -1, -1, 2, -1), 3),
+             "tail_bound": P(4, (0, 1, 3, 4), (0, 0, 1, 2), (-1, 0, -1, 2), None, 3),
+             "tail_distinct": P(4, (0, 1, 3, 4), (0, 0, 1, 2), (-1, 0, -1, -1), None, 3),
+             "tail_fixed": P(4, (0, 1, 3, 4), (0, 0, 1, 0), (-1, 0, 1, 1), None, 1)}
+    for name, p in list(PATTERNS.items()) + list(extra.items()):
+        off, cols = oracle_mod.rmat_graph(6, 8, 0x5EED7A06, oriented=(p.graph == "oriented"))
+        want = _pattern_brute_force(off, cols, p)
+        got = oracle_mod.pattern_count(off, cols, p.k, p.flags, p.offsets, p.backward,
+                                       p.restriction, p.reuse)
+        assert got == want, name
+
+
+def test_pattern_oracle_cliques(oracle_mod):
+    """Q0, Q3, Q5 and Q7 on the oriented graph are the 3-, 4-, 5- and
+    6-clique counts."""
+    from reset_b200.api import PATTERNS
+    off, cols = oracle_mod.rmat_graph(9, 16, 0x5EED7A09, oriented=True)
+    for name, k in (("Q0", 3), ("Q3", 4), ("Q5", 5), ("Q7", 6)):
+        p = PATTERNS[name]
+        got = oracle_mod.pattern_count(off, cols, p.k, p.flags, p.offsets, p.backward,
+                                       p.restriction, p.reuse)
+        assert got == oracle_mod.clique_k(off, cols, k), name
+
+
 def test_tc_counts_fixture_pins_small_scales(oracle_mod):
     """tests/golden/tc_counts.json (the oracle's exact counts of the
     benchmark's seeded graphs, which the GPU tests and bench.py assert) is
