@@ -22,7 +22,10 @@
 // is counted without a scan: the prefix length, or |C_l| less the earlier
 // vertices that a binary search finds in it.  Such a last level is not
 // entered at all: the level before it hands one candidate to each lane,
-// which counts the last level for it.  A reusing k-clique chain
+// which counts the last level for it.  A last level that intersects a fixed
+// vertex's row with the row of the candidate just picked (N(m_a) ∩ N(x))
+// is not entered either: such intersections of at most kLaneMax keys run
+// one candidate per lane, longer ones by the whole warp.  A reusing k-clique chain
 // without checks (SMOG's Q0, Q3, Q5, Q7) runs the k-clique kernel
 // (clique.cu).
 //
@@ -56,7 +59,13 @@ struct PatternDev {
   int32_t filt[kPatMax];           // 1: no later level reuses C_l
   int32_t chain;                   // a reusing clique chain without checks
   int32_t fuse;                    // the last level probes nothing
+  int32_t pair;                    // the last level lists {pair_a, k-2} only
+  int32_t pair_a;
 };
+
+// Intersections of the paired last level up to this length run one per
+// lane; longer ones take the whole warp.
+constexpr int kLaneMax = 32;
 
 // checkRestriction (SMOG/SMOG_hie/subgraph_match_hie.cu:23-42) with the
 // opposite sense: true when key x may be m_l.
@@ -111,7 +120,7 @@ __global__ void row_stats_kernel(const int32_t* __restrict__ off,
 }
 
 template <bool HIER>
-__global__ void __launch_bounds__(kPtThreads)
+__global__ void __launch_bounds__(kPtThreads, 5)
     pattern_kernel(const int4* __restrict__ desc, const int32_t* __restrict__ off,
                    const int32_t* __restrict__ cols, const int32_t* __restrict__ chunk_row,
                    int32_t n, int64_t m, const int32_t* __restrict__ table, int64_t bn, int b,
@@ -265,6 +274,63 @@ __global__ void __launch_bounds__(kPtThreads)
           continue;
         }
       }
+      if (sp.pair && lv == k - 2) {
+        // the last level is N(m_a) ∩ N(x) for the candidate x: short
+        // intersections run one candidate per lane (each lane holds its own
+        // m_lv = x in its copy of map), long ones afterwards by the warp
+        const int L = k - 1, rr = sp.restr[L];
+        const bool rcut = sorted && (sp.flags & RESET_PATTERN_RESTRICT) && rr >= 0;
+        const int4 da = __ldg(desc + map[sp.pair_a]);
+        for (int j0 = it[lv]; j0 < sz[lv]; j0 += 32) {
+          const int j = j0 + lane;
+          int x = j < sz[lv] ? cs[lv][j] : 0;
+          bool act = j < sz[lv];
+          if (act && (unsigned)x >= (unsigned)n) {
+            atomicOr(status, kErrBadId);
+            act = false;
+          }
+          act = act && level_ok(sp, lv, x, map);
+          int len = 0;
+          const int32_t* base = cols;
+          const int32_t* tb = table;
+          int tlg = 0;
+          if (act) {
+            const int4 dx = __ldg(desc + x);
+            const int4 db = dx.y <= da.y ? dx : da, dt = dx.y <= da.y ? da : dx;
+            base = cols + db.x;
+            len = dt.y > 0 ? db.y : 0;
+            tb = table + desc_toff(dt);
+            tlg = desc_lg(dt);
+            if (rcut) len = lower_bound_key(base, len, rr == lv ? x : map[rr]);
+          }
+          const bool big = len > kLaneMax;
+          if (!big && len > 0) {
+            map[lv] = x;
+            unsigned long long c = 0;
+            for (int t = 0; t < len; ++t) {
+              const int z = base[t];
+              c += level_ok(sp, L, z, map) && probe_key<HIER>(z, tb, tlg, lg_max, bn, b, status);
+            }
+            hits += c;
+          }
+          for (unsigned bm = __ballot_sync(kFull, big); bm; bm &= bm - 1) {
+            const int f = __ffs(bm) - 1;
+            const int xb = __shfl_sync(kFull, x, f);
+            const int lb = __shfl_sync(kFull, len, f);
+            const int32_t* bb = cols + __shfl_sync(kFull, (int)(base - cols), f);
+            const int4 dx = __ldg(desc + xb);
+            const int4 dt = dx.y <= da.y ? da : dx;
+            map[lv] = xb;
+            for (int t = lane; t < lb; t += 32) {
+              const int z = bb[t];
+              hits += level_ok(sp, L, z, map) &&
+                      probe_key<HIER>(z, table + desc_toff(dt), desc_lg(dt), lg_max, bn, b, status);
+            }
+          }
+        }
+        --lv;
+        continue;
+      }
       if (sorted && sp.fuse && lv == k - 2) {
         // the last level probes nothing: every key x of C_lv that passes
         // lv's check is m_lv for one lane, which counts the last level's
@@ -396,6 +462,14 @@ reset_status compile_pattern(const reset_pattern* p, PatternDev* d) {
   d->chain = chain ? 1 : 0;
   d->fuse = k >= 4 && ((d->reuse[k - 1] >= 0 && d->nb[k - 1] == 0) ||
                        (d->reuse[k - 1] < 0 && d->nb[k - 1] == 1));
+  d->pair = 0;
+  if (k >= 4 && d->reuse[k - 1] < 0 && d->nb[k - 1] == 2) {
+    const int a = d->back[k - 1][0], c = d->back[k - 1][1];
+    if ((a == k - 2) != (c == k - 2)) {
+      d->pair = 1;
+      d->pair_a = a == k - 2 ? c : a;
+    }
+  }
   return RESET_OK;
 }
 
