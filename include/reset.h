@@ -355,6 +355,14 @@ reset_status reset_pattern_count(const reset_table *t, const int32_t *d_off,
                                  const reset_pattern *p, uint64_t *d_count,
                                  reset_stream_t stream);
 
+/* SMOG's query patterns by name, "Q0" .. "Q8" (SMOG/SMOG_hie/
+ * script_hie.py:85-152): *out points at library-owned static arrays;
+ * *oriented (if not NULL) is 1 for the patterns SMOG counts on the oriented
+ * graph (Q0, Q3, Q5, Q7: begin.bin / adjacent.bin), 0 for those it counts
+ * on the symmetric one (generic_*.bin; SMOG/SMOG_hie/common_hie.cu:72-85).
+ * RESET_ERR_ARG for another name.  Host-only. */
+reset_status reset_pattern_named(const char *name, reset_pattern *out, int32_t *oriented);
+
 /* |A ∩ B| counted with A's multiplicity for one pair of device arrays
  * (keys >= 0).  Builds B's table with `params` and probes A.  *d_count
  * (device i64) is overwritten.  Replaces make_hashtable_kernel +

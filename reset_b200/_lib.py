@@ -107,6 +107,7 @@ SIGNATURES = {
     "reset_clique4_count": (I32, [P, P, P, I64, P, P]),
     "reset_clique_count": (I32, [P, P, P, I64, I32, P, P]),
     "reset_pattern_count": (I32, [P, P, P, I64, C.POINTER(Pattern), P, P]),
+    "reset_pattern_named": (I32, [C.c_char_p, C.POINTER(Pattern), C.POINTER(C.c_int32)]),
     "reset_sss": (I32, [P, P, P, P, P, I64, I32, I32, P, P, P]),
     "reset_sss_float": (I32, [P, P, P, P, P, I64, C.c_float, P, P, P]),
     "reset_ir": (I32, [P, P, P, P, P, I32, P, P, P, P]),

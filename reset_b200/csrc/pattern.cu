@@ -473,10 +473,56 @@ reset_status compile_pattern(const reset_pattern* p, PatternDev* d) {
   return RESET_OK;
 }
 
+// SMOG's query patterns (SMOG/SMOG_hie/script_hie.py:85-152) and the graph
+// each is counted on (SMOG/SMOG_hie/common_hie.cu:72-85).
+struct NamedPattern {
+  const char* name;
+  int32_t k, flags, oriented;
+  int32_t offsets[kPatMax], backward[2 * kPatMax], restriction[kPatMax], reuse[kPatMax];
+  bool has_restriction, has_reuse;
+};
+
+constexpr int32_t kRD = RESET_PATTERN_RESTRICT | RESET_PATTERN_DISTINCT;
+const NamedPattern kNamed[] = {
+    {"Q0", 3, 0, 1, {0, 1, 3}, {0, 0, 1}, {}, {}, false, false},
+    {"Q1", 4, RESET_PATTERN_RESTRICT, 0, {0, 1, 2, 4}, {0, 0, 1, 2}, {-1, 0, 1, 0}, {},
+     true, false},
+    {"Q2", 4, RESET_PATTERN_RESTRICT, 0, {0, 1, 3, 5}, {0, 0, 1, 1, 2}, {-1, -1, 1, 0}, {},
+     true, false},
+    {"Q3", 4, 0, 1, {0, 1, 3, 5}, {0, 0, 1, -1, 2}, {}, {-1, -1, -1, 2}, false, true},
+    {"Q4", 5, kRD, 0, {0, 1, 3, 5, 6}, {0, 0, 1, -1, 2, -1}, {-1, 0, -1, 2, -1},
+     {-1, -1, -1, 2, 2}, true, true},
+    {"Q5", 5, 0, 1, {0, 1, 3, 5, 7}, {0, 0, 1, -1, 2, -1, 3}, {}, {-1, -1, -1, 2, 3}, false,
+     true},
+    {"Q6", 5, kRD, 0, {0, 1, 3, 4, 6}, {0, 0, 1, -1, 2, 3}, {-1, 0, -1, 2, -1},
+     {-1, -1, -1, 2, -1}, true, true},
+    {"Q7", 6, 0, 1, {0, 1, 3, 5, 7, 9}, {0, 0, 1, -1, 2, -1, 3, -1, 4}, {},
+     {-1, -1, -1, 2, 3, 4}, false, true},
+    {"Q8", 5, RESET_PATTERN_RESTRICT, 0, {0, 1, 3, 5, 6}, {0, 0, 1, -1, 2, -1},
+     {-1, 0, -1, -1, 3}, {-1, -1, -1, 2, 3}, true, true},
+};
+
 }  // namespace
 }  // namespace rst
 
 using namespace rst;
+
+extern "C" reset_status reset_pattern_named(const char* name, reset_pattern* out,
+                                            int32_t* oriented) {
+  if (!name || !out) return arg_fail("NULL name or pattern");
+  for (const NamedPattern& q : kNamed) {
+    if (std::strcmp(q.name, name) != 0) continue;
+    out->k = q.k;
+    out->flags = q.flags;
+    out->offsets = q.offsets;
+    out->backward = q.backward;
+    out->restriction = q.has_restriction ? q.restriction : nullptr;
+    out->reuse = q.has_reuse ? q.reuse : nullptr;
+    if (oriented) *oriented = q.oriented;
+    return RESET_OK;
+  }
+  return arg_fail("unknown pattern name (SMOG's table has Q0..Q8)");
+}
 
 extern "C" reset_status reset_pattern_count(const reset_table* t, const int32_t* d_off,
                                             const int32_t* d_cols, int64_t m,

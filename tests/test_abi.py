@@ -178,3 +178,41 @@ def test_pattern_count_validates_on_the_host(libreset):
         api.pattern_struct(P(4, (0, 1, 3), (0, 0, 1)))
     with pytest.raises(ValueError):
         api.pattern_struct(P(3, (0, 1, 3), (0, 0, 1), (-1, 0)))
+
+
+def test_named_patterns_match_the_python_table(libreset):
+    """reset_pattern_named (the C copy of SMOG's Q0..Q8 table) holds the
+    same arrays, flags and graph choice as api.PATTERNS."""
+    from reset_b200 import _lib, api
+    for name, spec in api.PATTERNS.items():
+        ps, ori = _lib.Pattern(), ctypes.c_int32(-1)
+        assert libreset.reset_pattern_named(name.encode(), ctypes.byref(ps), ctypes.byref(ori)) == 0
+        assert (ps.k, ps.flags) == (spec.k, spec.flags), name
+        assert ori.value == (1 if spec.graph == "oriented" else 0), name
+        assert [ps.offsets[i] for i in range(ps.k)] == list(spec.offsets), name
+        nb = spec.offsets[-1]
+        assert [ps.backward[i] for i in range(nb)] == list(spec.backward[:nb]), name
+        for field in ("restriction", "reuse"):
+            want, ptr = getattr(spec, field), getattr(ps, field)
+            if want is None:
+                assert not ptr, (name, field)
+            else:
+                assert [ptr[i] for i in range(ps.k)] == list(want), (name, field)
+    assert libreset.reset_pattern_named(b"Q9", ctypes.byref(_lib.Pattern()), None) == 3
+    assert libreset.reset_pattern_named(None, ctypes.byref(_lib.Pattern()), None) == 3
+
+
+def test_smog_cli_rejects_bad_input_before_any_gpu_work(libreset, tmp_path):
+    """reset_smog checks the pattern name and its graph files on the host."""
+    import subprocess
+    exe = os.path.join(ROOT, "reset_b200", "bin", "reset_smog")
+    if not os.path.exists(exe):
+        from reset_b200 import build
+        build.build_host_tools()
+    r = subprocess.run([exe, str(tmp_path), "Q9"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "unknown pattern" in r.stderr
+    r = subprocess.run([exe, str(tmp_path / "missing"), "Q1"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1 and "cannot open file" in r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "Usage" in r.stderr

@@ -99,3 +99,34 @@ def test_reset_intersection_cli(cuda, libreset, tmp_path, name):
     out = run("reset_intersection", "--files", f"{tmp_path}/a.bin", f"{tmp_path}/b.bin")
     got = int(re.search(r"Intersection Result Count: (\d+)", out).group(1))
     assert got == g["ref_meta"][1]
+
+
+def _write_smog_graph(d, prefix, off, cols):
+    """SMOG's graph folder files (SMOG/SMOG_hie/common_hie.cu:61-129): raw
+    int32 arrays, no header."""
+    n = off.size - 1
+    vtx = np.repeat(np.arange(n, dtype=np.int32), np.diff(off))
+    for name, a in (("begin", off), ("adjacent", cols), ("vertex", vtx),
+                    ("md", [int(np.diff(off).max())])):
+        np.asarray(a, dtype=np.int32).tofile(f"{d}/{prefix}{name}.bin")
+
+
+def test_reset_smog_cli(cuda, libreset, oracle_mod, tmp_path):
+    """SMOG's executable interface: its graph folder (oriented files for the
+    clique patterns, generic_ ones for the rest), its positional arguments
+    and its result line, for every pattern of its table, against the
+    oracle's count by definition."""
+    from reset_b200.api import PATTERNS
+    d = str(tmp_path)
+    o_off, o_cols = oracle_mod.rmat_graph(9, 16, 0x5EED5309, oriented=True)
+    s_off, s_cols = oracle_mod.rmat_graph(9, 16, 0x5EED5309, oriented=False)
+    _write_smog_graph(d, "", o_off, o_cols)
+    _write_smog_graph(d, "generic_", s_off, s_cols)
+    for name, p in PATTERNS.items():
+        off, cols = (o_off, o_cols) if p.graph == "oriented" else (s_off, s_cols)
+        want = oracle_mod.pattern_count(off, cols, p.k, p.flags, p.offsets, p.backward,
+                                        p.restriction, p.reuse)
+        out = run("reset_smog", d, name, 1, 0.2, 5, 1024, 216, 1)
+        assert int(re.search(rf"{name} count is (\d+)", out).group(1)) == want, name
+        assert f"graph vertex number is : {off.size - 1}" in out
+        assert re.search(r"Hierarchical time: [0-9.e+-]+ ms", out)
