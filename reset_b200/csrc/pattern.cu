@@ -25,9 +25,9 @@
 // which counts the last level for it.  A last level that intersects a fixed
 // vertex's row with the row of the candidate just picked (N(m_a) ∩ N(x))
 // is not entered either: such intersections of at most kLaneMax keys run
-// one candidate per lane, longer ones by the whole warp.  A reusing k-clique chain
-// without checks (SMOG's Q0, Q3, Q5, Q7) runs the k-clique kernel
-// (clique.cu).
+// one candidate per lane, longer ones by the whole warp.  A reusing
+// k-clique chain without checks (SMOG's Q0, Q3, Q5, Q7) runs the k-clique
+// kernel (clique.cu).
 //
 // Semantics differ from the reference in one case only: where two listed
 // vertices of a level map to the same data vertex and that vertex has the
